@@ -1,0 +1,89 @@
+"""ctypes binding of liblbm_b200.so (the C ABI declared in include/lbm_b200.h).
+
+The library is built in-tree by ``cudalbm_b200/build.py`` into
+``cudalbm_b200/lib/liblbm_b200.so``.  Importing this module without the built
+library raises immediately: there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "liblbm_b200.so")
+
+LBM_OK = 0
+STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4: "device wait timed out",
+          5: "I/O error", 6: "parse error", 7: "invalid state", 8: "non-finite value in solution"}
+
+FO_S, FO_SMEAN, FO_K, FO_KMEAN, FO_MOMENTSMEAN = 1, 2, 4, 8, 16
+FO_BITS = {"S": FO_S, "SMean": FO_SMEAN, "k": FO_K, "kMean": FO_KMEAN, "momentsMean": FO_MOMENTSMEAN}
+
+FIELDS_MOMENTS, FIELDS_S, FIELDS_SMEAN, FIELDS_K, FIELDS_KMEAN, FIELDS_MOMENTSMEAN = range(6)
+FIELD_SET = {"moments": 0, "S": 1, "SMean": 2, "k": 3, "kMean": 4, "momentsMean": 5}
+ORDER_GLOBAL, ORDER_TILED = 0, 1
+F32, F64 = 0, 1
+
+# every symbol include/lbm_b200.h declares
+EXPORTS = ("lbm_config_default", "lbm_create", "lbm_destroy", "lbm_init_regions", "lbm_write_fields",
+           "lbm_read_fields", "lbm_step", "lbm_synchronize", "lbm_reduce", "lbm_get_info", "lbm_last_error",
+           "lbm_status_string", "lbm_field_set_vars")
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("lattice", ctypes.c_int32), ("device", ctypes.c_int32), ("nx", ctypes.c_int64),
+                ("ny", ctypes.c_int64), ("nz", ctypes.c_int64), ("Re", ctypes.c_float), ("u_inf", ctypes.c_float),
+                ("function_objects", ctypes.c_uint32), ("mean_bits", ctypes.c_int32),
+                ("start_step", ctypes.c_int64), ("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32),
+                ("z_chunk", ctypes.c_int32), ("stages", ctypes.c_int32)]
+
+
+class Info(ctypes.Structure):
+    _fields_ = [("step", ctypes.c_int64), ("nodes", ctypes.c_int64), ("tau", ctypes.c_float),
+                ("omega", ctypes.c_float), ("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32),
+                ("z_chunk", ctypes.c_int32), ("stages", ctypes.c_int32), ("device_bytes", ctypes.c_uint64),
+                ("last_step_ms", ctypes.c_double), ("kernel_launches", ctypes.c_uint64)]
+
+
+class LBMError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load the in-tree library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m cudalbm_b200.build` (needs nvcc)")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i32, u64, sz = ctypes.c_void_p, ctypes.c_int32, ctypes.c_uint64, ctypes.c_size_t
+        L.lbm_config_default.argtypes = [ctypes.POINTER(Config)]
+        L.lbm_config_default.restype = None
+        L.lbm_create.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(vp)]
+        L.lbm_destroy.argtypes = [vp]
+        L.lbm_init_regions.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
+        L.lbm_write_fields.argtypes = [vp, i32, vp, sz, i32, i32]
+        L.lbm_read_fields.argtypes = [vp, i32, vp, sz, i32, i32]
+        L.lbm_step.argtypes = [vp, u64]
+        L.lbm_synchronize.argtypes = [vp]
+        L.lbm_reduce.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+        L.lbm_get_info.argtypes = [vp, ctypes.POINTER(Info)]
+        L.lbm_last_error.restype = ctypes.c_char_p
+        L.lbm_status_string.restype = ctypes.c_char_p
+        L.lbm_status_string.argtypes = [i32]
+        L.lbm_field_set_vars.argtypes = [i32]
+        for name in ("lbm_create", "lbm_destroy", "lbm_init_regions", "lbm_write_fields", "lbm_read_fields",
+                     "lbm_step", "lbm_synchronize", "lbm_reduce", "lbm_get_info"):
+            getattr(L, name).restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != LBM_OK:
+        raise LBMError(status, lib().lbm_last_error().decode(errors="replace"))

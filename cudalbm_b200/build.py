@@ -1,0 +1,103 @@
+"""In-tree build of the native parts (no GPU needed: nvcc cross-compiles).
+
+    python -m cudalbm_b200.build            # library + solver executables
+    python -m cudalbm_b200.build --force    # rebuild everything
+
+Outputs:
+  cudalbm_b200/lib/liblbm_b200.so      C ABI of include/lbm_b200.h (sm_100a)
+  cudalbm_b200/bin/momentBasedD3Q19    solver executables with the reference's
+  cudalbm_b200/bin/momentBasedD3Q27    command line and case files
+"""
+from __future__ import annotations
+
+import glob
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+LIB = os.path.join(HERE, "lib", "liblbm_b200.so")
+BIN = os.path.join(HERE, "bin")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-cudart", "static",
+              "-I" + INCLUDE, "-I" + CSRC] + ARCH
+
+LIB_SOURCES = ["lbm_capi.cu"]
+HOST_SOURCES = ["casefile.cpp", "lbmbin.cpp"]
+
+
+def _nvcc() -> str:
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _stale(target: str, deps) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _deps():
+    return sorted(glob.glob(os.path.join(CSRC, "*")) + glob.glob(os.path.join(INCLUDE, "*.h")))
+
+
+def _run(cmd):
+    print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def build_library(force: bool = False, verbose_ptxas: bool = False) -> str:
+    srcs = [os.path.join(CSRC, s) for s in LIB_SOURCES]
+    if force or _stale(LIB, _deps()):
+        os.makedirs(os.path.dirname(LIB), exist_ok=True)
+        cmd = [_nvcc()] + NVCC_FLAGS + ["-shared"] + srcs + ["-o", LIB + ".tmp"]
+        if verbose_ptxas:
+            cmd += ["-Xptxas", "-v"]
+        _run(cmd)
+        os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+def build_executables(force: bool = False) -> list:
+    out = []
+    main = os.path.join(CSRC, "solver_main.cpp")
+    if not os.path.exists(main):
+        return out
+    os.makedirs(BIN, exist_ok=True)
+    host = [os.path.join(CSRC, s) for s in HOST_SOURCES if os.path.exists(os.path.join(CSRC, s))]
+    for q in (19, 27):
+        exe = os.path.join(BIN, f"momentBasedD3Q{q}")
+        if force or _stale(exe, _deps() + [LIB]):
+            _run([_nvcc(), "-std=c++17", "-O2", "-I" + INCLUDE, "-I" + CSRC, f"-DLBM_LATTICE={q}", main] + host +
+                 ["-o", exe, "-L" + os.path.dirname(LIB), "-llbm_b200", "-Xlinker", "-rpath=$ORIGIN/../lib"])
+        out.append(exe)
+    return out
+
+
+def build_oracle() -> None:
+    """CPU oracle (test infrastructure) and, where the reference sources are
+    present, the reference executables used as the parity checker."""
+    _run(["make", "-s", "-f", os.path.join(ROOT, "oracle", "Makefile")])
+    ref = os.environ.get("LBM_REFERENCE_DIR", "/root/reference")
+    if os.path.isdir(os.path.join(ref, "applications")):
+        _run(["make", "-s", "-f", os.path.join(ROOT, "oracle", "Makefile.ref"), f"REF={ref}"])
+
+
+def build(force: bool = False) -> None:
+    build_library(force)
+    build_executables(force)
+
+
+if __name__ == "__main__":
+    force = "--force" in sys.argv
+    build(force)
+    if "--oracle" in sys.argv:
+        build_oracle()

@@ -1,0 +1,717 @@
+// lbm_capi.cu -- implementation of the C ABI in include/lbm_b200.h.
+//
+// Owns the device state of one cavity (two moment buffers, the function-object
+// accumulators, the TMA descriptors and a stream), dispatches the fused step
+// kernel of lbm_step.cuh and provides the device-side helpers around it:
+// initial state from region values, host<->device transfers in either node
+// order, and double-precision global reductions.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <type_traits>
+#include <utility>
+#include <vector>
+
+#include "lbm_b200.h"
+#include "lbm_step.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+lbm_status fail(lbm_status s, const std::string &msg)
+{
+    g_last_error = msg;
+    return s;
+}
+
+#define LBM_CUDA(call)                                                                                        \
+    do {                                                                                                      \
+        cudaError_t e_ = (call);                                                                              \
+        if (e_ != cudaSuccess)                                                                                \
+            return fail(e_ == cudaErrorMemoryAllocation ? LBM_ERR_NOMEM : LBM_ERR_CUDA,                      \
+                        std::string(#call) + ": " + cudaGetErrorString(e_) + " (" + std::to_string((int)e_) + ")"); \
+    } while (0)
+
+// ---------------------------------------------------------------- kernels
+__global__ void init_regions_kernel(float *m, int nx, int ny, int nz, const float *region)
+{
+    // src/array/hostArray.cuh:304-359, evaluated in float as the reference does
+    // (its "front" is z == 0 and "back" z == nz-1 there).
+    const size_t N = size_t(nx) * ny * nz;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x) {
+        const int x = int(i % nx), y = int((i / nx) % ny), z = int(i / (size_t(nx) * ny));
+        const bool w = x == 0, e = x == nx - 1, s = y == 0, n = y == ny - 1, fr = z == 0, b = z == nz - 1;
+        const int count = w + e + s + n + fr + b;
+#pragma unroll
+        for (int f = 0; f < 10; f++) {
+            const float *r = region + 7 * f;
+            const float sum = (float(w) * r[4]) + (float(e) * r[3]) + (float(s) * r[2]) + (float(n) * r[1]) +
+                              (float(fr) * r[5]) + (float(b) * r[6]);
+            m[f * N + i] = count > 0 ? sum / float(count) : r[0];
+        }
+    }
+}
+
+__device__ __forceinline__ size_t tiled_index(int x, int y, int z, int nbx, int nby)
+{
+    const int tx = x & 7, ty = y & 7, tz = z & 7, bx = x >> 3, by = y >> 3, bz = z >> 3;
+    return size_t(tx) + 8 * (size_t(ty) + 8 * (size_t(tz) + 8 * (size_t(bx) + size_t(nbx) * (size_t(by) + size_t(nby) * bz))));
+}
+
+// dst (device layout, global order) <- src (one field of nodes, given order/type)
+template <typename S, typename D>
+__global__ void gather_in_kernel(D *dst, const S *src, int nx, int ny, int nz, int tiled)
+{
+    const size_t N = size_t(nx) * ny * nz;
+    const int nbx = nx / 8, nby = ny / 8;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x) {
+        const int x = int(i % nx), y = int((i / nx) % ny), z = int(i / (size_t(nx) * ny));
+        const size_t j = tiled ? tiled_index(x, y, z, nbx, nby) : i;
+        dst[i] = D(src[j]);
+    }
+}
+template <typename S, typename D>
+__global__ void scatter_out_kernel(D *dst, const S *src, int nx, int ny, int nz, int tiled)
+{
+    const size_t N = size_t(nx) * ny * nz;
+    const int nbx = nx / 8, nby = ny / 8;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x) {
+        const int x = int(i % nx), y = int((i / nx) % ny), z = int(i / (size_t(nx) * ny));
+        const size_t j = tiled ? tiled_index(x, y, z, nbx, nby) : i;
+        dst[j] = D(src[i]);
+    }
+}
+
+__global__ void reduce_kernel(const float *m, size_t N, double *acc, unsigned long long *bad)
+{
+    double mass = 0.0, ke = 0.0;
+    unsigned long long nb = 0;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x) {
+        const double rho = double(m[i]) + 1.0;
+        const double u = double(m[N + i]) / 3.0, v = double(m[2 * N + i]) / 3.0, w = double(m[3 * N + i]) / 3.0;
+        mass += rho;
+        ke += 0.5 * rho * (u * u + v * v + w * w);
+#pragma unroll
+        for (int f = 0; f < 10; f++)
+            nb += !isfinite(m[f * N + i]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mass += __shfl_down_sync(0xffffffffu, mass, o);
+        ke += __shfl_down_sync(0xffffffffu, ke, o);
+        nb += __shfl_down_sync(0xffffffffu, nb, o);
+    }
+    __shared__ double s_m[32], s_k[32];
+    __shared__ unsigned long long s_b[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        s_m[wid] = mass;
+        s_k[wid] = ke;
+        s_b[wid] = nb;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = blockDim.x >> 5;
+        mass = lane < nw ? s_m[lane] : 0.0;
+        ke = lane < nw ? s_k[lane] : 0.0;
+        nb = lane < nw ? s_b[lane] : 0ull;
+        for (int o = 16; o > 0; o >>= 1) {
+            mass += __shfl_down_sync(0xffffffffu, mass, o);
+            ke += __shfl_down_sync(0xffffffffu, ke, o);
+            nb += __shfl_down_sync(0xffffffffu, nb, o);
+        }
+        if (lane == 0) {
+            atomicAdd(&acc[0], mass);
+            atomicAdd(&acc[1], ke);
+            atomicAdd(bad, nb);
+        }
+    }
+}
+
+// --------------------------------------------------------- kernel table
+using lbm::StepParams;
+
+struct TileCfg {
+    int tx, ty, stages;
+};
+
+template <int Q, int TX, int TY, int NS, bool FO, typename MeanT>
+struct KernelInst {
+    static constexpr size_t smem = lbm::SmemLayout<Q, TX, TY, NS>::bytes;
+    static void *fn() { return reinterpret_cast<void *>(&lbm::step_kernel<Q, TX, TY, NS, FO, MeanT>); }
+};
+
+struct Launcher {
+    void *fn = nullptr;
+    size_t smem = 0;
+    int tx = 0, ty = 0, stages = 0;
+};
+
+template <int Q, int TX, int TY, int NS>
+Launcher pick_fo(bool fo, int mean_bits)
+{
+    Launcher l;
+    l.tx = TX;
+    l.ty = TY;
+    l.stages = NS;
+    if (!fo) {
+        l.fn = KernelInst<Q, TX, TY, NS, false, float>::fn();
+        l.smem = KernelInst<Q, TX, TY, NS, false, float>::smem;
+    } else if (mean_bits == 64) {
+        l.fn = KernelInst<Q, TX, TY, NS, true, double>::fn();
+        l.smem = KernelInst<Q, TX, TY, NS, true, double>::smem;
+    } else {
+        l.fn = KernelInst<Q, TX, TY, NS, true, float>::fn();
+        l.smem = KernelInst<Q, TX, TY, NS, true, float>::smem;
+    }
+    return l;
+}
+
+// Available tile shapes.  The first entry per lattice is the default for
+// large meshes; narrower tiles serve meshes whose nx is not a multiple of 32.
+bool pick_launcher(int Q, int tx, int ty, int stages, bool fo, int mean_bits, Launcher &out)
+{
+#define LBM_TRY(QQ, TXX, TYY, NSS)                          \
+    if (Q == QQ && tx == TXX && ty == TYY && stages == NSS) { \
+        out = pick_fo<QQ, TXX, TYY, NSS>(fo, mean_bits);      \
+        return true;                                          \
+    }
+    LBM_TRY(19, 32, 8, 3)
+    LBM_TRY(19, 16, 8, 3)
+    LBM_TRY(19, 8, 8, 3)
+    LBM_TRY(27, 32, 8, 2)
+    LBM_TRY(27, 16, 8, 2)
+    LBM_TRY(27, 8, 8, 2)
+#undef LBM_TRY
+    return false;
+}
+
+// Default tiling for a mesh: widest tile whose width divides nx, z-chunks
+// sized so that the grid holds several waves of CTAs on 148 SMs.
+void default_tiling(int Q, int64_t nx, int64_t ny, int64_t nz, int &tx, int &ty, int &zc, int &stages)
+{
+    tx = (nx % 32 == 0) ? 32 : (nx % 16 == 0 ? 16 : 8);
+    ty = 8;
+    stages = Q == 19 ? 3 : 2;
+    const int64_t tiles = ((nx + tx - 1) / tx) * ((ny + ty - 1) / ty);
+    int64_t c = nz;
+    while (c > 16 && tiles * ((nz + c - 1) / c) < 8 * 148)
+        c = (c + 1) / 2;
+    zc = int(c);
+}
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn get_encode()
+{
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+}  // namespace
+
+struct lbm_handle {
+    lbm_config cfg{};
+    int Q = 19;
+    size_t N = 0;
+    cudaStream_t stream = nullptr;
+    float *m[2] = {nullptr, nullptr};
+    int cur = 0;
+    CUtensorMap tmap[2];
+    // function objects
+    float *S = nullptr, *k = nullptr;
+    void *SMean = nullptr, *kMean = nullptr, *momentsMean = nullptr;
+    unsigned *err = nullptr;
+    double *red = nullptr;
+    void *scratch = nullptr;
+    size_t scratch_bytes = 0;
+    float tau = 0, omega = 0, t_omega = 0, omega_d2 = 0;
+    int64_t t = 0;
+    Launcher launcher;
+    int zc = 0;
+    uint64_t device_bytes = 0;
+    uint64_t launches = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool timed = false;
+};
+
+namespace {
+
+template <typename T>
+lbm_status dev_alloc(lbm_handle *h, T **p, size_t count)
+{
+    LBM_CUDA(cudaMalloc(reinterpret_cast<void **>(p), count * sizeof(T)));
+    h->device_bytes += count * sizeof(T);
+    return LBM_OK;
+}
+
+lbm_status make_tmap(lbm_handle *h, int which)
+{
+    EncodeTiledFn enc = get_encode();
+    if (!enc)
+        return fail(LBM_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    const auto &c = h->cfg;
+    const int XPAD = 4;
+    cuuint64_t dims[4] = {cuuint64_t(c.nx), cuuint64_t(c.ny), cuuint64_t(c.nz), 10};
+    cuuint64_t strides[3] = {cuuint64_t(c.nx) * 4, cuuint64_t(c.nx) * c.ny * 4, cuuint64_t(h->N) * 4};
+    cuuint32_t box[4] = {cuuint32_t(h->launcher.tx + 2 * XPAD), cuuint32_t(h->launcher.ty + 2), 1, 10};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = enc(&h->tmap[which], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->m[which], dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return fail(LBM_ERR_CUDA, "cuTensorMapEncodeTiled failed with CUresult " + std::to_string(int(r)));
+    return LBM_OK;
+}
+
+int nvars_of(lbm_field_set s)
+{
+    switch (s) {
+    case LBM_FIELDS_MOMENTS: return 10;
+    case LBM_FIELDS_S: return 6;
+    case LBM_FIELDS_SMEAN: return 6;
+    case LBM_FIELDS_K: return 1;
+    case LBM_FIELDS_KMEAN: return 1;
+    case LBM_FIELDS_MOMENTSMEAN: return 10;
+    }
+    return -1;
+}
+
+// device pointer and element type (0 float, 1 double) of a field set
+lbm_status field_ptr(lbm_handle *h, lbm_field_set s, void **p, int *is_double)
+{
+    const bool md = h->cfg.mean_bits == 64;
+    *is_double = 0;
+    switch (s) {
+    case LBM_FIELDS_MOMENTS: *p = h->m[h->cur]; break;
+    case LBM_FIELDS_S: *p = h->S; break;
+    case LBM_FIELDS_SMEAN: *p = h->SMean; *is_double = md; break;
+    case LBM_FIELDS_K: *p = h->k; break;
+    case LBM_FIELDS_KMEAN: *p = h->kMean; *is_double = md; break;
+    case LBM_FIELDS_MOMENTSMEAN: *p = h->momentsMean; *is_double = md; break;
+    default: return fail(LBM_ERR_ARG, "unknown field set");
+    }
+    if (!*p)
+        return fail(LBM_ERR_STATE, "field set not enabled for this handle (see function_objects)");
+    return LBM_OK;
+}
+
+lbm_status ensure_scratch(lbm_handle *h, size_t bytes)
+{
+    if (h->scratch_bytes >= bytes)
+        return LBM_OK;
+    if (h->scratch) {
+        cudaFree(h->scratch);
+        h->device_bytes -= h->scratch_bytes;
+        h->scratch = nullptr;
+        h->scratch_bytes = 0;
+    }
+    LBM_CUDA(cudaMalloc(&h->scratch, bytes));
+    h->scratch_bytes = bytes;
+    h->device_bytes += bytes;
+    return LBM_OK;
+}
+
+dim3 grid_1d(size_t N)
+{
+    return dim3(unsigned(std::min<size_t>((N + 255) / 256, size_t(148) * 16)));
+}
+
+template <typename MeanT>
+lbm_status launch_step(lbm_handle *h)
+{
+    StepParams<MeanT> p{};
+    const int nxt = h->cur ^ 1;
+    p.out = h->m[nxt];
+    p.nx = int(h->cfg.nx);
+    p.ny = int(h->cfg.ny);
+    p.nz = int(h->cfg.nz);
+    p.zc = h->zc;
+    p.rx = lbm::Relax{h->omega, h->t_omega, h->omega_d2, h->tau, h->cfg.u_inf};
+    p.fo.S = h->S;
+    p.fo.SMean = static_cast<MeanT *>(h->SMean);
+    p.fo.k = h->k;
+    p.fo.kMean = static_cast<MeanT *>(h->kMean);
+    p.fo.momentsMean = static_cast<MeanT *>(h->momentsMean);
+    // invNewCount = 1 / (timeStep + 1) in scalar_t (strainRateTensor.cuh:332)
+    if constexpr (std::is_same_v<MeanT, float>)
+        p.fo.inv_count = 1.0f / static_cast<float>(h->t + 1);
+    else
+        p.fo.inv_count = 1.0 / static_cast<double>(h->t + 1);
+    p.err = h->err;
+    p.timeout_ns = 2000000000ull;
+    const dim3 block(h->launcher.tx, h->launcher.ty);
+    const dim3 grid(unsigned((h->cfg.nx + h->launcher.tx - 1) / h->launcher.tx),
+                    unsigned((h->cfg.ny + h->launcher.ty - 1) / h->launcher.ty),
+                    unsigned((h->cfg.nz + h->zc - 1) / h->zc));
+    void *args[] = {&h->tmap[h->cur], &p};
+    LBM_CUDA(cudaLaunchKernel(h->launcher.fn, grid, block, args, h->launcher.smem, h->stream));
+    h->cur = nxt;
+    h->t += 1;
+    h->launches += 1;
+    return LBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void lbm_config_default(lbm_config *c)
+{
+    std::memset(c, 0, sizeof(*c));
+    c->lattice = 19;
+    c->device = 0;
+    c->nx = c->ny = c->nz = 64;
+    c->Re = 100.0f;
+    c->u_inf = 0.05f;
+    c->function_objects = 0;
+    c->mean_bits = 32;
+    c->start_step = 0;
+}
+
+const char *lbm_last_error(void) { return g_last_error.c_str(); }
+
+const char *lbm_status_string(lbm_status s)
+{
+    switch (s) {
+    case LBM_OK: return "ok";
+    case LBM_ERR_ARG: return "invalid argument";
+    case LBM_ERR_CUDA: return "CUDA error";
+    case LBM_ERR_NOMEM: return "out of memory";
+    case LBM_ERR_TIMEOUT: return "device wait timed out";
+    case LBM_ERR_IO: return "I/O error";
+    case LBM_ERR_PARSE: return "parse error";
+    case LBM_ERR_STATE: return "invalid state";
+    case LBM_ERR_NONFINITE: return "non-finite value in solution";
+    }
+    return "unknown status";
+}
+
+int lbm_field_set_vars(lbm_field_set set) { return nvars_of(set); }
+
+lbm_status lbm_create(const lbm_config *cfg, lbm_handle **out)
+{
+    g_last_error.clear();
+    if (!cfg || !out)
+        return fail(LBM_ERR_ARG, "null argument");
+    *out = nullptr;
+    const lbm_config &c = *cfg;
+    if (c.lattice != 19 && c.lattice != 27)
+        return fail(LBM_ERR_ARG, "lattice must be 19 or 27");
+    if (c.nx <= 0 || c.ny <= 0 || c.nz <= 0 || c.nx % 8 || c.ny % 8 || c.nz % 8)
+        return fail(LBM_ERR_ARG, "mesh dimensions must be positive multiples of 8 (block::nx() * nxBlocks() == nx)");
+    if (c.nx > (1 << 30) || c.ny > (1 << 30) || c.nz > (1 << 30))
+        return fail(LBM_ERR_ARG, "mesh dimension too large");
+    if (!(c.Re > 0.0f) || !std::isfinite(c.u_inf))
+        return fail(LBM_ERR_ARG, "Re must be positive and u_inf finite");
+    if (c.mean_bits != 32 && c.mean_bits != 64)
+        return fail(LBM_ERR_ARG, "mean_bits must be 32 or 64");
+    if (c.function_objects & ~0x1Fu)
+        return fail(LBM_ERR_ARG, "unknown function object bits");
+
+    int ndev = 0;
+    LBM_CUDA(cudaGetDeviceCount(&ndev));
+    if (c.device < 0 || c.device >= ndev)
+        return fail(LBM_ERR_ARG, "device ordinal out of range (Number of GPUs requested is greater than the number available)");
+    LBM_CUDA(cudaSetDevice(c.device));
+
+    lbm_handle *h = new lbm_handle();
+    h->cfg = c;
+    h->Q = c.lattice;
+    h->N = size_t(c.nx) * c.ny * c.nz;
+    h->t = c.start_step;
+
+    // relaxation constants in float, as the reference (latticeMesh.cuh:177-201)
+    const float nu = c.u_inf * static_cast<float>(c.nx - 1) / c.Re;
+    h->tau = 0.5f + 3.0f * nu;
+    h->omega = 1.0f / h->tau;
+    h->t_omega = 1.0f - h->omega;
+    h->omega_d2 = h->omega * 0.5f;
+
+    int tx, ty, zc, st;
+    default_tiling(h->Q, c.nx, c.ny, c.nz, tx, ty, zc, st);
+    if (c.tile_x) tx = c.tile_x;
+    if (c.tile_y) ty = c.tile_y;
+    if (c.z_chunk) zc = c.z_chunk;
+    if (c.stages) st = c.stages;
+    const bool fo = c.function_objects != 0;
+    if (!pick_launcher(h->Q, tx, ty, st, fo, c.mean_bits, h->launcher)) {
+        delete h;
+        return fail(LBM_ERR_ARG, "unsupported tile configuration");
+    }
+    h->zc = std::max(1, std::min<int>(zc, int(c.nz)));
+
+    auto cleanup_fail = [&](lbm_status s) {
+        std::string msg = g_last_error;
+        lbm_destroy(h);
+        g_last_error = msg;
+        return s;
+    };
+    lbm_status s;
+    LBM_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    LBM_CUDA(cudaEventCreate(&h->ev0));
+    LBM_CUDA(cudaEventCreate(&h->ev1));
+    for (int b = 0; b < 2; b++)
+        if ((s = dev_alloc(h, &h->m[b], 10 * h->N)) != LBM_OK)
+            return cleanup_fail(s);
+    const size_t msz = c.mean_bits == 64 ? 8 : 4;
+    if (c.function_objects & LBM_FO_S)
+        if ((s = dev_alloc(h, &h->S, 6 * h->N)) != LBM_OK) return cleanup_fail(s);
+    if (c.function_objects & LBM_FO_K)
+        if ((s = dev_alloc(h, &h->k, h->N)) != LBM_OK) return cleanup_fail(s);
+    if (c.function_objects & LBM_FO_SMEAN)
+        if ((s = dev_alloc(h, reinterpret_cast<char **>(&h->SMean), 6 * h->N * msz)) != LBM_OK) return cleanup_fail(s);
+    if (c.function_objects & LBM_FO_KMEAN)
+        if ((s = dev_alloc(h, reinterpret_cast<char **>(&h->kMean), h->N * msz)) != LBM_OK) return cleanup_fail(s);
+    if (c.function_objects & LBM_FO_MOMENTSMEAN)
+        if ((s = dev_alloc(h, reinterpret_cast<char **>(&h->momentsMean), 10 * h->N * msz)) != LBM_OK) return cleanup_fail(s);
+    if ((s = dev_alloc(h, &h->err, 4)) != LBM_OK) return cleanup_fail(s);
+    if ((s = dev_alloc(h, &h->red, 4)) != LBM_OK) return cleanup_fail(s);
+    for (int b = 0; b < 2; b++) {
+        cudaMemsetAsync(h->m[b], 0, 10 * h->N * 4, h->stream);
+    }
+    if (h->S) cudaMemsetAsync(h->S, 0, 6 * h->N * 4, h->stream);
+    if (h->k) cudaMemsetAsync(h->k, 0, h->N * 4, h->stream);
+    if (h->SMean) cudaMemsetAsync(h->SMean, 0, 6 * h->N * msz, h->stream);
+    if (h->kMean) cudaMemsetAsync(h->kMean, 0, h->N * msz, h->stream);
+    if (h->momentsMean) cudaMemsetAsync(h->momentsMean, 0, 10 * h->N * msz, h->stream);
+    cudaMemsetAsync(h->err, 0, 4, h->stream);
+    if (cudaGetLastError() != cudaSuccess)
+        return cleanup_fail(fail(LBM_ERR_CUDA, "cudaMemsetAsync failed"));
+    for (int b = 0; b < 2; b++)
+        if ((s = make_tmap(h, b)) != LBM_OK)
+            return cleanup_fail(s);
+    if (cudaFuncSetAttribute(h->launcher.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(h->launcher.smem)) != cudaSuccess)
+        return cleanup_fail(fail(LBM_ERR_CUDA, "cannot reserve shared memory for the step kernel"));
+    *out = h;
+    return LBM_OK;
+}
+
+lbm_status lbm_destroy(lbm_handle *h)
+{
+    if (!h)
+        return LBM_OK;
+    cudaSetDevice(h->cfg.device);
+    if (h->stream)
+        cudaStreamSynchronize(h->stream);
+    for (void *p : {static_cast<void *>(h->m[0]), static_cast<void *>(h->m[1]), static_cast<void *>(h->S),
+                    static_cast<void *>(h->k), h->SMean, h->kMean, h->momentsMean, static_cast<void *>(h->err),
+                    static_cast<void *>(h->red), h->scratch})
+        if (p)
+            cudaFree(p);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream)
+        cudaStreamDestroy(h->stream);
+    delete h;
+    return LBM_OK;
+}
+
+lbm_status lbm_init_regions(lbm_handle *h, const float region[70])
+{
+    if (!h || !region)
+        return fail(LBM_ERR_ARG, "null argument");
+    LBM_CUDA(cudaSetDevice(h->cfg.device));
+    lbm_status s = ensure_scratch(h, 70 * sizeof(float));
+    if (s != LBM_OK)
+        return s;
+    LBM_CUDA(cudaMemcpyAsync(h->scratch, region, 70 * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    init_regions_kernel<<<grid_1d(h->N), 256, 0, h->stream>>>(h->m[h->cur], int(h->cfg.nx), int(h->cfg.ny),
+                                                               int(h->cfg.nz), static_cast<float *>(h->scratch));
+    LBM_CUDA(cudaGetLastError());
+    h->launches += 1;
+    const size_t msz = h->cfg.mean_bits == 64 ? 8 : 4;
+    if (h->S) cudaMemsetAsync(h->S, 0, 6 * h->N * 4, h->stream);
+    if (h->k) cudaMemsetAsync(h->k, 0, h->N * 4, h->stream);
+    if (h->SMean) cudaMemsetAsync(h->SMean, 0, 6 * h->N * msz, h->stream);
+    if (h->kMean) cudaMemsetAsync(h->kMean, 0, h->N * msz, h->stream);
+    if (h->momentsMean) cudaMemsetAsync(h->momentsMean, 0, 10 * h->N * msz, h->stream);
+    LBM_CUDA(cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+lbm_status lbm_write_fields(lbm_handle *h, lbm_field_set set, const void *host, size_t count, lbm_dtype dtype,
+                            lbm_order order)
+{
+    if (!h || !host)
+        return fail(LBM_ERR_ARG, "null argument");
+    const int nv = nvars_of(set);
+    if (nv < 0)
+        return fail(LBM_ERR_ARG, "unknown field set");
+    if (count != size_t(nv) * h->N)
+        return fail(LBM_ERR_ARG, "count must equal nvars * nx * ny * nz");
+    if (order == LBM_ORDER_TILED && (h->cfg.nx % 8 || h->cfg.ny % 8 || h->cfg.nz % 8))
+        return fail(LBM_ERR_ARG, "tiled order needs multiples of 8");
+    LBM_CUDA(cudaSetDevice(h->cfg.device));
+    void *dptr;
+    int is_double;
+    lbm_status s = field_ptr(h, set, &dptr, &is_double);
+    if (s != LBM_OK)
+        return s;
+    const size_t hsz = dtype == LBM_F64 ? 8 : 4;
+    if ((s = ensure_scratch(h, h->N * hsz)) != LBM_OK)
+        return s;
+    const int tiled = order == LBM_ORDER_TILED;
+    for (int v = 0; v < nv; v++) {
+        const char *src = static_cast<const char *>(host) + size_t(v) * h->N * hsz;
+        LBM_CUDA(cudaMemcpyAsync(h->scratch, src, h->N * hsz, cudaMemcpyHostToDevice, h->stream));
+        const int nx = int(h->cfg.nx), ny = int(h->cfg.ny), nz = int(h->cfg.nz);
+        if (dtype == LBM_F64) {
+            if (is_double)
+                gather_in_kernel<double, double><<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<double *>(dptr) + v * h->N, static_cast<const double *>(h->scratch), nx, ny, nz, tiled);
+            else
+                gather_in_kernel<double, float><<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<float *>(dptr) + v * h->N, static_cast<const double *>(h->scratch), nx, ny, nz, tiled);
+        } else {
+            if (is_double)
+                gather_in_kernel<float, double><<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<double *>(dptr) + v * h->N, static_cast<const float *>(h->scratch), nx, ny, nz, tiled);
+            else
+                gather_in_kernel<float, float><<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<float *>(dptr) + v * h->N, static_cast<const float *>(h->scratch), nx, ny, nz, tiled);
+        }
+        LBM_CUDA(cudaGetLastError());
+        h->launches += 1;
+    }
+    LBM_CUDA(cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+lbm_status lbm_read_fields(lbm_handle *h, lbm_field_set set, void *host, size_t count, lbm_dtype dtype, lbm_order order)
+{
+    if (!h || !host)
+        return fail(LBM_ERR_ARG, "null argument");
+    const int nv = nvars_of(set);
+    if (nv < 0)
+        return fail(LBM_ERR_ARG, "unknown field set");
+    if (count != size_t(nv) * h->N)
+        return fail(LBM_ERR_ARG, "count must equal nvars * nx * ny * nz");
+    LBM_CUDA(cudaSetDevice(h->cfg.device));
+    void *dptr;
+    int is_double;
+    lbm_status s = field_ptr(h, set, &dptr, &is_double);
+    if (s != LBM_OK)
+        return s;
+    const size_t hsz = dtype == LBM_F64 ? 8 : 4;
+    const size_t dsz = is_double ? 8 : 4;
+    const int tiled = order == LBM_ORDER_TILED;
+    const bool direct = !tiled && hsz == dsz;
+    if (!direct && (s = ensure_scratch(h, h->N * hsz)) != LBM_OK)
+        return s;
+    const int nx = int(h->cfg.nx), ny = int(h->cfg.ny), nz = int(h->cfg.nz);
+    for (int v = 0; v < nv; v++) {
+        char *dst = static_cast<char *>(host) + size_t(v) * h->N * hsz;
+        const char *src = static_cast<const char *>(dptr) + size_t(v) * h->N * dsz;
+        if (direct) {
+            LBM_CUDA(cudaMemcpyAsync(dst, src, h->N * hsz, cudaMemcpyDeviceToHost, h->stream));
+            continue;
+        }
+        if (dtype == LBM_F64) {
+            if (is_double)
+                scatter_out_kernel<double, double><<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<double *>(h->scratch), reinterpret_cast<const double *>(src), nx, ny, nz, tiled);
+            else
+                scatter_out_kernel<float, double><<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<double *>(h->scratch), reinterpret_cast<const float *>(src), nx, ny, nz, tiled);
+        } else {
+            if (is_double)
+                scatter_out_kernel<double, float><<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<float *>(h->scratch), reinterpret_cast<const double *>(src), nx, ny, nz, tiled);
+            else
+                scatter_out_kernel<float, float><<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<float *>(h->scratch), reinterpret_cast<const float *>(src), nx, ny, nz, tiled);
+        }
+        LBM_CUDA(cudaGetLastError());
+        h->launches += 1;
+        LBM_CUDA(cudaMemcpyAsync(dst, h->scratch, h->N * hsz, cudaMemcpyDeviceToHost, h->stream));
+    }
+    LBM_CUDA(cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+lbm_status lbm_step(lbm_handle *h, uint64_t n)
+{
+    if (!h)
+        return fail(LBM_ERR_ARG, "null handle");
+    LBM_CUDA(cudaSetDevice(h->cfg.device));
+    if (n == 0)
+        return LBM_OK;
+    LBM_CUDA(cudaEventRecord(h->ev0, h->stream));
+    const bool md = h->cfg.mean_bits == 64;
+    for (uint64_t i = 0; i < n; i++) {
+        lbm_status s = md ? launch_step<double>(h) : launch_step<float>(h);
+        if (s != LBM_OK)
+            return s;
+    }
+    LBM_CUDA(cudaEventRecord(h->ev1, h->stream));
+    h->timed = true;
+    return LBM_OK;
+}
+
+lbm_status lbm_synchronize(lbm_handle *h)
+{
+    if (!h)
+        return fail(LBM_ERR_ARG, "null handle");
+    LBM_CUDA(cudaSetDevice(h->cfg.device));
+    LBM_CUDA(cudaStreamSynchronize(h->stream));
+    unsigned e = 0;
+    LBM_CUDA(cudaMemcpy(&e, h->err, 4, cudaMemcpyDeviceToHost));
+    if (e & lbm::ERR_TMA_TIMEOUT)
+        return fail(LBM_ERR_TIMEOUT, "a step kernel timed out waiting for a TMA copy");
+    return LBM_OK;
+}
+
+lbm_status lbm_reduce(lbm_handle *h, double out[3])
+{
+    if (!h || !out)
+        return fail(LBM_ERR_ARG, "null argument");
+    LBM_CUDA(cudaSetDevice(h->cfg.device));
+    LBM_CUDA(cudaMemsetAsync(h->red, 0, 4 * sizeof(double), h->stream));
+    reduce_kernel<<<grid_1d(h->N), 256, 0, h->stream>>>(h->m[h->cur], h->N, h->red,
+                                                         reinterpret_cast<unsigned long long *>(h->red + 2));
+    LBM_CUDA(cudaGetLastError());
+    h->launches += 1;
+    double r[3];
+    unsigned long long bad = 0;
+    LBM_CUDA(cudaMemcpyAsync(r, h->red, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    LBM_CUDA(cudaMemcpyAsync(&bad, h->red + 2, sizeof(bad), cudaMemcpyDeviceToHost, h->stream));
+    LBM_CUDA(cudaStreamSynchronize(h->stream));
+    out[0] = r[0];
+    out[1] = r[1];
+    out[2] = double(bad);
+    return LBM_OK;
+}
+
+lbm_status lbm_get_info(lbm_handle *h, lbm_info *info)
+{
+    if (!h || !info)
+        return fail(LBM_ERR_ARG, "null argument");
+    std::memset(info, 0, sizeof(*info));
+    info->step = h->t;
+    info->nodes = int64_t(h->N);
+    info->tau = h->tau;
+    info->omega = h->omega;
+    info->tile_x = h->launcher.tx;
+    info->tile_y = h->launcher.ty;
+    info->z_chunk = h->zc;
+    info->stages = h->launcher.stages;
+    info->device_bytes = h->device_bytes;
+    info->kernel_launches = h->launches;
+    if (h->timed) {
+        float ms = 0.0f;
+        if (cudaEventSynchronize(h->ev1) == cudaSuccess && cudaEventElapsedTime(&ms, h->ev0, h->ev1) == cudaSuccess)
+            info->last_step_ms = ms;
+    }
+    return LBM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,119 @@
+"""Python front end of the solver: one lid-driven cavity on one GPU.
+
+Mirrors what the reference executables do in ``main``
+(applications/momentBasedD3Q19/momentBasedD3Q19.cu:56-140): read a case,
+set up the state, step, write .LBMBin snapshots.  All compute goes through the
+C ABI (include/lbm_b200.h); this module only marshals host buffers.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Dict, Iterable, Optional
+
+import numpy as np
+
+from . import _lib
+from .casefiles import MOMENT_NAMES, lid_cavity_values, scaled_region_values
+
+FIELD_NAMES = {
+    "moments": list(MOMENT_NAMES),
+    "S": ["S_xx", "S_xy", "S_xz", "S_yy", "S_yz", "S_zz"],
+    "SMean": ["S_xxMean", "S_xyMean", "S_xzMean", "S_yyMean", "S_yzMean", "S_zzMean"],
+    "k": ["k"],
+    "kMean": ["kMean"],
+    "momentsMean": [n + "Mean" for n in MOMENT_NAMES],
+}
+NVARS = {k: len(v) for k, v in FIELD_NAMES.items()}
+
+
+class Cavity:
+    """Device state of one cavity behind an ``lbm_handle``."""
+
+    def __init__(self, lattice: int, nx: int, ny: int, nz: int, Re: float, u_inf: float,
+                 function_objects: Iterable[str] = (), mean_bits: int = 32, device: int = 0,
+                 start_step: int = 0, tile: Optional[tuple] = None, z_chunk: int = 0):
+        L = _lib.lib()
+        cfg = _lib.Config()
+        L.lbm_config_default(ctypes.byref(cfg))
+        cfg.lattice, cfg.device = int(lattice), int(device)
+        cfg.nx, cfg.ny, cfg.nz = int(nx), int(ny), int(nz)
+        cfg.Re, cfg.u_inf = float(Re), float(u_inf)
+        self.function_objects = list(function_objects)
+        mask = 0
+        for name in self.function_objects:
+            mask |= _lib.FO_BITS[name]
+        cfg.function_objects = mask
+        cfg.mean_bits = int(mean_bits)
+        cfg.start_step = int(start_step)
+        if tile:
+            cfg.tile_x, cfg.tile_y = int(tile[0]), int(tile[1])
+            if len(tile) > 2:
+                cfg.stages = int(tile[2])
+        cfg.z_chunk = int(z_chunk)
+        self.cfg = cfg
+        self.shape = (nz, ny, nx)
+        self.mean_bits = mean_bits
+        h = ctypes.c_void_p()
+        _lib.check(L.lbm_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+
+    # ------------------------------------------------------------ lifecycle
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.lib().lbm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -------------------------------------------------------------- state
+    def init_regions(self, region_values=None) -> None:
+        """Initial state from per-region values (default: the lid cavity)."""
+        if region_values is None:
+            region_values = scaled_region_values(lid_cavity_values(self.cfg.u_inf))
+        rv = np.ascontiguousarray(region_values, dtype=np.float32).reshape(70)
+        _lib.check(_lib.lib().lbm_init_regions(self._h, rv.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+
+    def write(self, data: np.ndarray, field_set: str = "moments", tiled: bool = False) -> None:
+        data = np.ascontiguousarray(data)
+        dtype = _lib.F64 if data.dtype == np.float64 else _lib.F32
+        if data.dtype not in (np.float32, np.float64):
+            data = data.astype(np.float32)
+        _lib.check(_lib.lib().lbm_write_fields(self._h, _lib.FIELD_SET[field_set], data.ctypes.data, data.size,
+                                               dtype, _lib.ORDER_TILED if tiled else _lib.ORDER_GLOBAL))
+
+    def read(self, field_set: str = "moments", dtype=np.float32, tiled: bool = False, out=None) -> np.ndarray:
+        nv = NVARS[field_set]
+        nz, ny, nx = self.shape
+        shape = (nv, nx * ny * nz) if tiled else (nv, nz, ny, nx)
+        if out is None:
+            out = np.empty(shape, dtype=dtype)
+        _lib.check(_lib.lib().lbm_read_fields(self._h, _lib.FIELD_SET[field_set], out.ctypes.data, out.size,
+                                              _lib.F64 if out.dtype == np.float64 else _lib.F32,
+                                              _lib.ORDER_TILED if tiled else _lib.ORDER_GLOBAL))
+        return out
+
+    def step(self, n: int = 1) -> None:
+        _lib.check(_lib.lib().lbm_step(self._h, int(n)))
+
+    def synchronize(self) -> None:
+        _lib.check(_lib.lib().lbm_synchronize(self._h))
+
+    def reduce(self) -> Dict[str, float]:
+        out = (ctypes.c_double * 3)()
+        _lib.check(_lib.lib().lbm_reduce(self._h, out))
+        return {"mass": out[0], "kinetic_energy": out[1], "nonfinite": int(out[2])}
+
+    def info(self) -> Dict[str, object]:
+        inf = _lib.Info()
+        _lib.check(_lib.lib().lbm_get_info(self._h, ctypes.byref(inf)))
+        return {f: getattr(inf, f) for f, _ in inf._fields_}

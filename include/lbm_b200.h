@@ -1,0 +1,155 @@
+/*
+ * lbm_b200.h -- C ABI of the B200 moment-representation LBM solver.
+ *
+ * The reference (geoenergiaUDESC/cudaLBM) compiles its hot path into each
+ * executable as header-only templates and exposes no library interface; its
+ * observable surface is the executables momentBasedD3Q19 / momentBasedD3Q27,
+ * the case files and the .LBMBin output.  This header is the boundary that
+ * replaces the reference's in-process pieces: every entry point below names
+ * the reference code it stands in for.  Plain C types only; the library owns
+ * all device memory; callers pass host buffers.  Every call returns an
+ * lbm_status; nothing inside the library exits the process (the reference's
+ * checkCudaErrors calls std::exit, src/errorHandler.cuh:88-111).
+ *
+ * Threading: a handle belongs to one host thread at a time and owns one CUDA
+ * stream.  Different handles may be used from different threads.
+ */
+#ifndef LBM_B200_H
+#define LBM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_B200_ABI_VERSION 1
+
+typedef enum lbm_status {
+    LBM_OK = 0,
+    LBM_ERR_ARG = 1,      /* invalid argument / size (reference: errorHandler(ERR_SIZE, ...)) */
+    LBM_ERR_CUDA = 2,     /* CUDA runtime error (reference: std::exit(cudaError)) */
+    LBM_ERR_NOMEM = 3,    /* device or host allocation failed */
+    LBM_ERR_TIMEOUT = 4,  /* a bounded device wait gave up (kernel reported, context intact) */
+    LBM_ERR_IO = 5,       /* file missing, unreadable, truncated or unwritable */
+    LBM_ERR_PARSE = 6,    /* malformed case file (reference: uncaught std::runtime_error) */
+    LBM_ERR_STATE = 7,    /* call not valid in the handle's current state */
+    LBM_ERR_NONFINITE = 8 /* a NaN/Inf was found in the solution */
+} lbm_status;
+
+/* Function objects (reference src/functionObjects/*, switched on by the
+ * functionObjects case file). Bit mask. */
+enum {
+    LBM_FO_S = 1u << 0,          /* strain-rate tensor, 6 components */
+    LBM_FO_SMEAN = 1u << 1,      /* running mean of S */
+    LBM_FO_K = 1u << 2,          /* k = 0.5*sqrt(u^2+v^2+w^2) of the stored (scaled) velocity */
+    LBM_FO_KMEAN = 1u << 3,      /* running mean of k */
+    LBM_FO_MOMENTSMEAN = 1u << 4 /* running mean of the 10 stored moments */
+};
+
+/* Field sets for lbm_read_fields / lbm_write_fields. */
+typedef enum lbm_field_set {
+    LBM_FIELDS_MOMENTS = 0,     /* rho-1, u, v, w, m_xx, m_xy, m_xz, m_yy, m_yz, m_zz (scaled, as stored) */
+    LBM_FIELDS_S = 1,           /* S_xx, S_xy, S_xz, S_yy, S_yz, S_zz */
+    LBM_FIELDS_SMEAN = 2,       /* S_xxMean ... S_zzMean */
+    LBM_FIELDS_K = 3,           /* k */
+    LBM_FIELDS_KMEAN = 4,       /* kMean */
+    LBM_FIELDS_MOMENTSMEAN = 5  /* rhoMean ... m_zzMean */
+} lbm_field_set;
+
+/* Node order of host buffers. */
+typedef enum lbm_order {
+    LBM_ORDER_GLOBAL = 0, /* [field][z][y][x], x fastest */
+    LBM_ORDER_TILED = 1   /* [field][reference block-tiled index]: tx + 8*(ty + 8*(tz + 8*(bx + NBX*(by + NBY*bz))))
+                             (reference src/globalFunctions.cuh:208-214; the .LBMBin data order) */
+} lbm_order;
+
+/* Host value types for field transfers. */
+typedef enum lbm_dtype { LBM_F32 = 0, LBM_F64 = 1 } lbm_dtype;
+
+typedef struct lbm_config {
+    int32_t lattice;          /* 19 (D3Q19) or 27 (D3Q27) */
+    int32_t device;           /* CUDA device ordinal (the reference's -GPU argument, deviceList()[0]) */
+    int64_t nx, ny, nz;       /* lattice size; each a multiple of 8 (reference latticeMesh.cuh:115-131) */
+    float Re;                 /* Reynolds number (programControl) */
+    float u_inf;              /* lid speed, U_North = {u_inf, 0, 0} (latticeMesh.cuh:183) */
+    uint32_t function_objects;/* LBM_FO_* mask */
+    int32_t mean_bits;        /* 32: float running means as the reference; 64: double accumulators */
+    int64_t start_step;       /* absolute step index of the initial state (restart: latestTime) */
+    /* kernel tiling; 0 = autotuned choice for this size class */
+    int32_t tile_x, tile_y, z_chunk, stages;
+} lbm_config;
+
+typedef struct lbm_handle lbm_handle;
+
+typedef struct lbm_info {
+    int64_t step;            /* absolute step index of the next step to run */
+    int64_t nodes;           /* nx*ny*nz */
+    float tau, omega;        /* relaxation constants as uploaded (latticeMesh.cuh:177-201) */
+    int32_t tile_x, tile_y, z_chunk, stages;
+    uint64_t device_bytes;   /* device memory owned by the handle */
+    double last_step_ms;     /* device time of the last lbm_step call (CUDA events) */
+    uint64_t kernel_launches;/* kernels launched by this handle so far */
+} lbm_info;
+
+/* Fill *cfg with defaults (D3Q19, 64^3, Re 100, u_inf 0.05, no function objects).
+ * Replaces: nothing (convenience). */
+void lbm_config_default(lbm_config *cfg);
+
+/* Allocate device state for one cavity and upload the relaxation constants.
+ * Replaces host::latticeMesh (src/latticeMesh/latticeMesh.cuh:85-210), the
+ * device::array allocations (momentBasedD3Q19.cu:70-79), device::halo
+ * (src/blockHalo/halo.cuh:76-122) and objectRegistry allocation
+ * (src/functionObjects/objectRegistry.cuh:78-87). */
+lbm_status lbm_create(const lbm_config *cfg, lbm_handle **out);
+
+/* Release everything the handle owns. */
+lbm_status lbm_destroy(lbm_handle *h);
+
+/* Initial state on the device from per-region values: region[f*7 + r] for
+ * fields f in moment order and regions r = internalField, North, South, East,
+ * West, Front, Back, already scaled (rho as rho-1, u*3, m_aa*4.5, m_ab*9).
+ * Replaces host::array::initialConditions (src/array/hostArray.cuh:304-359)
+ * and the host-side halo fill (src/blockHalo/haloFace.cuh:244-306). Function-
+ * object accumulators are zeroed. */
+lbm_status lbm_init_regions(lbm_handle *h, const float region[70]);
+
+/* Upload a field set from host memory (restart from .LBMBin, hostArray.cuh:264-276).
+ * `count` = number of values (nvars * nodes). */
+lbm_status lbm_write_fields(lbm_handle *h, lbm_field_set set, const void *host, size_t count, lbm_dtype dtype,
+                            lbm_order order);
+
+/* Download a field set to host memory (host::toHost, src/memory/memory.cuh:157-195). */
+lbm_status lbm_read_fields(lbm_handle *h, lbm_field_set set, void *host, size_t count, lbm_dtype dtype,
+                           lbm_order order);
+
+/* Advance n time steps (the momentBasedD3Q19<<<>>> launch + runTimeObjects.calculate
+ * + blockHalo.swap of momentBasedD3Q19.cu:104-137, with the function objects fused
+ * into the step kernel and no host synchronisation between steps).
+ * Asynchronous: returns after enqueueing; errors of the launches are reported. */
+lbm_status lbm_step(lbm_handle *h, uint64_t n);
+
+/* Wait for queued work and report device-side error flags. */
+lbm_status lbm_synchronize(lbm_handle *h);
+
+/* Global sums in double precision over all nodes: out[0] = sum(rho) (mass),
+ * out[1] = sum(0.5*rho*|u|^2) with physical u = stored/3, out[2] = number of
+ * non-finite values in the 10 moment fields.  Device-side reduction. */
+lbm_status lbm_reduce(lbm_handle *h, double out[3]);
+
+lbm_status lbm_get_info(lbm_handle *h, lbm_info *info);
+
+/* Message of the last failure on this thread (empty if none). */
+const char *lbm_last_error(void);
+
+/* Human-readable name of a status code. */
+const char *lbm_status_string(lbm_status s);
+
+/* Number of nodes a field set holds per node (1, 6 or 10). */
+int lbm_field_set_vars(lbm_field_set set);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LBM_B200_H */
