@@ -1,0 +1,384 @@
+#!/usr/bin/env python
+"""Benchmark of the fused moment-representation LBM step on B200.
+
+    python bench.py [--gpus N --steps K --warmup W] [--workload NAME] [--impl reference]
+
+Default workload: D3Q27 lid-driven cavity, 256^3 nodes, Re = 1000,
+u_lid = 0.05, with the function objects S, SMean, k and kMean updated every
+step (FP32 storage, arithmetic and means, as the reference).  One step = one
+time step of the whole cavity.  Prints one JSON line (rank 0).
+
+* value       MLUPS of the device-timed step loop (CUDA events on the solver's
+              stream, inputs resident in HBM; the moment buffers, 1.3 GB, are
+              far larger than the 126 MB L2, so no flush is needed).
+* e2e         the same metric through the C ABI with host buffers: upload of
+              the state from pinned host memory, K x (lbm_step + lbm_reduce,
+              whose 24-byte result is read back every step), download of the
+              moments and function objects -- all inside the timed region.
+* roofline    algorithmic bytes per node update (reference tiling: 134 B for
+              D3Q27 + 4 + 24 + 48 + 8 B for k, S, SMean, kMean = 218 B) times
+              the nodes per launch over the measured launch time, against the
+              measured HBM copy bandwidth.
+* cpu_baseline  the FP64 OpenMP CPU oracle (oracle/, a restatement of the
+              reference's scheme; the reference has no CPU path) timed on this
+              host on the same mesh for a bounded number of steps.
+
+Multi-GPU: the cavity does not shard here ("replicas only"): every rank runs
+its own cavity, no data-path collective; value = all ranks' node updates over
+the slowest rank's time.
+
+--impl reference runs the reference's own solver, built from its sources into
+oracle/_ref (its only implementation is CUDA), on the same case, timing K steps
+after W from its per-step progress lines.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MLUPS and % HBM roofline (D3Q19/27 cavity); closure vs plain at equal error"
+
+# B_alg: algorithmic bytes per node update at the reference tiling (8^3 blocks):
+# moments 2*10*4 B + halo faces 2*0.75*QF*4 B (+ function-object traffic).
+WORKLOADS = {
+    "q27_256_fo": dict(lattice=27, n=(256, 256, 256), Re=1000.0, u=0.05, fo=("S", "SMean", "k", "kMean"),
+                       mean_bits=32, b_alg=218,
+                       desc="D3Q27 lid-driven cavity 256^3, Re=1000, u_lid=0.05, function objects S/SMean/k/kMean "
+                            "every step (FP32 means)"),
+    "q19_64": dict(lattice=19, n=(64, 64, 64), Re=100.0, u=0.05, fo=(), mean_bits=32, b_alg=110,
+                   desc="D3Q19 lid-driven cavity 64^3, Re=100, u_lid=0.05"),
+    "q19_256": dict(lattice=19, n=(256, 256, 256), Re=1000.0, u=0.05, fo=(), mean_bits=32, b_alg=110,
+                    desc="D3Q19 lid-driven cavity 256^3, Re=1000, u_lid=0.05"),
+    "q27_256": dict(lattice=27, n=(256, 256, 256), Re=1000.0, u=0.05, fo=(), mean_bits=32, b_alg=134,
+                    desc="D3Q27 lid-driven cavity 256^3, Re=1000, u_lid=0.05"),
+    "q19_512": dict(lattice=19, n=(512, 512, 512), Re=1000.0, u=0.05, fo=(), mean_bits=32, b_alg=110,
+                    desc="D3Q19 lid-driven cavity 512^3, Re=1000, u_lid=0.05"),
+    "q27_256_fo64": dict(lattice=27, n=(256, 256, 256), Re=1000.0, u=0.05, fo=("S", "SMean", "k", "kMean"),
+                         mean_bits=64, b_alg=274,
+                         desc="D3Q27 lid-driven cavity 256^3, Re=1000, function objects with FP64 means"),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# --------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.25)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        mhz, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    mhz.append(float(parts[1]))
+                    mx = float(parts[2])
+                except ValueError:
+                    continue
+                for nm, val in zip(names, parts[5:9]):
+                    if val.lower() == "active":
+                        reasons.add(nm)
+        os.unlink(self.path)
+        if not mhz:
+            return None
+        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def physical_gpu_index(local: int) -> int:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [v for v in vis.split(",") if v.strip()]
+        if local < len(ids) and ids[local].strip().isdigit():
+            return int(ids[local])
+    return local
+
+
+def hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_per_node(workload: str):
+    """DRAM bytes per node update of the step kernel from a committed ncu
+    capture summary (profiles/traffic.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
+            return float(json.load(fh)[workload]["dram_bytes_per_node"])
+    except Exception:
+        return None
+
+
+# ----------------------------------------------------------- CPU oracle
+def cpu_baseline(w, budget_s: float = 12.0):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    from pyoracle import Oracle
+
+    from cudalbm_b200 import casefiles
+
+    nx, ny, nz = w["n"]
+    o = Oracle(w["lattice"], nx, ny, nz, w["Re"], w["u"])
+    m = o.initial(casefiles.scaled_region_values(casefiles.lid_cavity_values(w["u"])))
+    fo = o.new_function_objects(w["fo"])
+    t0 = time.perf_counter()
+    o.run(m, 1, 0, fo)
+    one = time.perf_counter() - t0
+    steps = max(1, min(5, int(budget_s / max(one, 1e-6)) - 1))
+    t0 = time.perf_counter()
+    o.run(m, steps, 1, fo)
+    dt = time.perf_counter() - t0
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": round(nx * ny * nz * steps / dt / 1e6, 3), "unit": "MLUPS", "cores": cores, "kind": "port",
+            "sample": f"FP64 OpenMP oracle, {w['desc']}, {steps} steps after 1 untimed"}
+
+
+# ------------------------------------------------------------ our arm
+def run_ours(args, w):
+    import numpy as np
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if dist is None:
+            return v
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    from cudalbm_b200 import _lib
+    from cudalbm_b200.solver import NVARS, Cavity
+
+    nx, ny, nz = w["n"]
+    nodes = nx * ny * nz
+    cav = Cavity(w["lattice"], nx, ny, nz, w["Re"], w["u"], function_objects=w["fo"], mean_bits=w["mean_bits"],
+                 device=local)
+    cav.init_regions()
+    cav.step(args.warmup)
+    cav.synchronize()
+
+    # ---- device-timed loop (value)
+    sampler = ClockSampler(physical_gpu_index(local))
+    sampler.start()
+    barrier()
+    cav.synchronize()
+    launches0 = cav.info()["kernel_launches"]
+    cav.step(args.steps)
+    cav.synchronize()
+    barrier()
+    info = cav.info()
+    clocks = sampler.stop()
+    ms = max_over_ranks(info["last_step_ms"])
+    launches = info["kernel_launches"] - launches0
+    ms_step = ms / args.steps
+    value = world * nodes * args.steps / (ms / 1e3) / 1e6
+
+    # ---- end to end through the C ABI with pinned host buffers (e2e)
+    state = _lib.PinnedArray((10, nz, ny, nx), np.float32)
+    cav.read("moments", out=state.array)
+    outs = {fs: _lib.PinnedArray((NVARS[fs], nz, ny, nx), np.float64 if (w["mean_bits"] == 64 and "Mean" in fs)
+                                 else np.float32) for fs in ("moments",) + tuple(w["fo"])}
+    barrier()
+    cav.synchronize()
+    t0 = time.perf_counter()
+    cav.write(state.array)
+    for _ in range(args.steps):
+        cav.step(1)
+        cav.reduce()
+    for fs, buf in outs.items():
+        cav.read(fs, out=buf.array)
+    t1 = time.perf_counter()
+    barrier()
+    e2e_s = max_over_ranks(t1 - t0)
+    e2e = world * nodes * args.steps / e2e_s / 1e6
+    h2d = 10 * nodes * 4
+    d2h = sum(b.array.nbytes for b in outs.values())
+    red = cav.reduce()
+    cav.close()
+
+    if rank != 0:
+        return None
+    peak, peak_kind = hbm_peak()
+    achieved = w["b_alg"] * nodes / (ms_step / 1e3) / 1e9
+    tpn = traffic_per_node(args.workload)
+    line = {
+        "metric": METRIC,
+        "value": round(value, 2),
+        "unit": "MLUPS",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_step, 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic: the lid-driven cavity initial state generated from the case's region values",
+        "config": {"workload": w["desc"], "lattice": f"D3Q{w['lattice']}", "nx": nx, "ny": ny, "nz": nz,
+                   "Re": w["Re"], "u_lid": w["u"], "function_objects": list(w["fo"]),
+                   "mean_bits": w["mean_bits"], "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (moment buffers %.2f GB vs 126 MB L2); no flush" % (2 * 40 * nodes / 1e9)},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": (round(tpn * nodes) if tpn else None),
+                     "bytes_per_node_alg": w["b_alg"], "peak_kind": f"of {peak_kind}"},
+        "e2e": {"value": round(e2e, 2), "unit": "MLUPS", "h2d_bytes_per_step": round(h2d / args.steps),
+                "d2h_bytes_per_step": round(24 + d2h / args.steps),
+                "what": "lbm_write_fields (pinned h2d) + K x (lbm_step + lbm_reduce with its 24 B read back) + "
+                        "lbm_read_fields of moments and function objects"},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "check": {"mass": red["mass"], "nonfinite": red["nonfinite"]},
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(w)
+        except Exception as exc:  # reported, never silent
+            line["cpu_baseline"] = {"value": None, "error": repr(exc)}
+    return line
+
+
+# ------------------------------------------------------- reference arm
+def run_reference(args, w):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    from cudalbm_b200 import casefiles
+
+    exe = os.path.join(ROOT, "oracle", "_ref", f"momentBasedD3Q{w['lattice']}")
+    if not os.path.exists(exe):
+        return {"impl": "reference", "unavailable": f"{exe} not built (make -f oracle/Makefile.ref needs the "
+                                                    "reference sources)"}
+    nx, ny, nz = w["n"]
+    nodes = nx * ny * nz
+    W, K = args.warmup, args.steps
+    spec = casefiles.CaseSpec(nx=nx, ny=ny, nz=nz, Re=w["Re"], u_inf=w["u"], n_steps=W + K + 1,
+                              save_interval=W + K + 10, info_interval=1, function_objects=w["fo"])
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    with tempfile.TemporaryDirectory() as case:
+        casefiles.write_case(case, spec)
+        sampler = ClockSampler(physical_gpu_index(local))
+        proc = subprocess.Popen([exe, "-GPU", str(local)], cwd=case, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
+                                text=True, bufsize=1)
+        stamps = {}
+        tail = []
+        clocks = None
+        for line in proc.stdout:
+            now = time.perf_counter()
+            tail = (tail + [line])[-20:]
+            if line.startswith("Time: "):
+                t = int(line.split()[1])
+                stamps[t] = now
+                if t == W:
+                    sampler.start()
+                if t == W + K:
+                    clocks = sampler.stop()
+        rc = proc.wait()
+    if rc != 0 or W not in stamps or W + K not in stamps:
+        return {"impl": "reference", "unavailable": f"reference exited {rc}: {''.join(tail)[-300:]!r}"}
+    dt = (stamps[W + K] - stamps[W]) / K
+    value = nodes / dt / 1e6
+    return {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": round(value, 2),
+        "unit": "MLUPS",
+        "n_gpus": 1,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": round(dt * 1e3, 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic: the same lid-driven cavity case directory",
+        "config": {"workload": w["desc"], "lattice": f"D3Q{w['lattice']}", "nx": nx, "ny": ny, "nz": nz,
+                   "Re": w["Re"], "u_lid": w["u"], "function_objects": list(w["fo"]), "parallelism": "1 GPU"},
+        "cpu_baseline": {"value": round(value, 2), "unit": "MLUPS", "cores": 1, "kind": "reference",
+                         "sample": f"the reference's own executable (oracle/_ref/momentBasedD3Q{w['lattice']}, built "
+                                   "from its sources for sm_100a) on the B200 -- its only implementation is CUDA; "
+                                   f"{K} steps after {W}, timed by its per-step 'Time:' lines (wall clock, the "
+                                   "reference synchronises the device every step)"},
+        "e2e": {"value": round(value, 2), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clocks,
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--workload", default="q27_256_fo", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    w = WORKLOADS[args.workload]
+    line = run_reference(args, w) if args.impl == "reference" else run_ours(args, w)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

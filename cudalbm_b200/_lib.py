@@ -27,7 +27,7 @@ F32, F64 = 0, 1
 # every symbol include/lbm_b200.h declares
 EXPORTS = ("lbm_config_default", "lbm_create", "lbm_destroy", "lbm_init_regions", "lbm_write_fields",
            "lbm_read_fields", "lbm_step", "lbm_synchronize", "lbm_reduce", "lbm_get_info", "lbm_last_error",
-           "lbm_status_string", "lbm_field_set_vars")
+           "lbm_status_string", "lbm_field_set_vars", "lbm_host_alloc", "lbm_host_free")
 
 
 class Config(ctypes.Structure):
@@ -77,8 +77,10 @@ def lib() -> ctypes.CDLL:
         L.lbm_status_string.restype = ctypes.c_char_p
         L.lbm_status_string.argtypes = [i32]
         L.lbm_field_set_vars.argtypes = [i32]
+        L.lbm_host_alloc.argtypes = [sz, ctypes.POINTER(vp)]
+        L.lbm_host_free.argtypes = [vp]
         for name in ("lbm_create", "lbm_destroy", "lbm_init_regions", "lbm_write_fields", "lbm_read_fields",
-                     "lbm_step", "lbm_synchronize", "lbm_reduce", "lbm_get_info"):
+                     "lbm_step", "lbm_synchronize", "lbm_reduce", "lbm_get_info", "lbm_host_alloc", "lbm_host_free"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -87,3 +89,30 @@ def lib() -> ctypes.CDLL:
 def check(status: int) -> None:
     if status != LBM_OK:
         raise LBMError(status, lib().lbm_last_error().decode(errors="replace"))
+
+
+class PinnedArray:
+    """numpy view of page-locked host memory from lbm_host_alloc."""
+
+    def __init__(self, shape, dtype=None):
+        import numpy as np
+
+        dtype = np.dtype(dtype or np.float32)
+        n = int(np.prod(shape)) * dtype.itemsize
+        p = ctypes.c_void_p()
+        check(lib().lbm_host_alloc(max(n, 1), ctypes.byref(p)))
+        self._p = p
+        buf = (ctypes.c_char * max(n, 1)).from_address(p.value)
+        self.array = np.frombuffer(buf, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
+
+    def free(self):
+        if self._p:
+            self.array = None
+            lib().lbm_host_free(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

@@ -691,6 +691,22 @@ lbm_status lbm_reduce(lbm_handle *h, double out[3])
     return LBM_OK;
 }
 
+lbm_status lbm_host_alloc(size_t bytes, void **out)
+{
+    if (!out)
+        return fail(LBM_ERR_ARG, "null argument");
+    *out = nullptr;
+    LBM_CUDA(cudaMallocHost(out, bytes));
+    return LBM_OK;
+}
+
+lbm_status lbm_host_free(void *p)
+{
+    if (p)
+        LBM_CUDA(cudaFreeHost(p));
+    return LBM_OK;
+}
+
 lbm_status lbm_get_info(lbm_handle *h, lbm_info *info)
 {
     if (!h || !info)

@@ -277,7 +277,7 @@ __device__ __forceinline__ void interior_moments(const float *f, float *mom)
 
 // Wet-node boundary moments (unscaled), boundaryConditions.cuh:99-533.
 template <int Q>
-__device__ __noinline__ void boundary_moments(const float *f, unsigned t, const Relax &rx, float *mom)
+__device__ __forceinline__ void boundary_moments(const float *f, unsigned t, const Relax &rx, float *mom)
 {
     float mask[Q];
     fill_mask<Q>(mask, t);

@@ -38,7 +38,7 @@ typedef enum lbm_status {
     LBM_ERR_NONFINITE = 8 /* a NaN/Inf was found in the solution */
 } lbm_status;
 
-/* Function objects (reference src/functionObjects/*, switched on by the
+/* Function objects (reference src/functionObjects, switched on by the
  * functionObjects case file). Bit mask. */
 enum {
     LBM_FO_S = 1u << 0,          /* strain-rate tensor, 6 components */
@@ -139,6 +139,12 @@ lbm_status lbm_synchronize(lbm_handle *h);
 lbm_status lbm_reduce(lbm_handle *h, double out[3]);
 
 lbm_status lbm_get_info(lbm_handle *h, lbm_info *info);
+
+/* Page-locked host memory for fast transfers (cudaMallocHost); free with
+ * lbm_host_free.  Replaces: the reference's pinned host::array variant
+ * (src/array/hostArray.cuh:66-140). */
+lbm_status lbm_host_alloc(size_t bytes, void **out);
+lbm_status lbm_host_free(void *p);
 
 /* Message of the last failure on this thread (empty if none). */
 const char *lbm_last_error(void);

@@ -1,0 +1,198 @@
+"""Parity of the CUDA step with the reference solver and the FP64 oracle.
+
+The kernel evaluates every node update with the reference's expressions in
+the same order, so on the same inputs its output is bit-for-bit the
+reference's.  The checks below therefore compare raw bit patterns against
+(a) the committed golden outputs of the reference executables, (b) the
+reference executables run live on this GPU (oracle/_ref, when built), and the
+stated tolerance (relative L2 per moment <= 1e-5) is met with margin: it is
+exactly 0.  Against the FP64 oracle the difference is the reference's own
+FP32 rounding (see test_oracle_golden.py).
+"""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from cudalbm_b200 import casefiles, lbmbin
+from cudalbm_b200.solver import Cavity
+from helpers import GOLDEN_CASES, lattice_q, load_golden, max_abs, rel_l2, spec_of
+
+from pyoracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_TOL = 1e-5  # stated bar: relative L2 per moment against the reference
+
+
+def bits_equal(a, b):
+    return np.array_equal(np.asarray(a, np.float32).view(np.uint32), np.asarray(b, np.float32).view(np.uint32))
+
+
+def run_cavity(q, nx, ny, nz, Re, u, steps, fo=(), region=None, **kw):
+    c = Cavity(q, nx, ny, nz, Re, u, function_objects=fo, **kw)
+    c.init_regions(region)
+    c.step(steps)
+    c.synchronize()
+    out = {"moments": c.read("moments")}
+    for f in fo:
+        out[f] = c.read(f)
+    c.close()
+    return out
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_bitwise_equal_to_reference_golden(name):
+    meta, arr = load_golden(name)
+    s = meta["spec"]
+    rv = casefiles.scaled_region_values(spec_of(meta).initial_values())
+    out = run_cavity(lattice_q(meta), s["nx"], s["ny"], s["nz"], s["Re"], s["u_inf"], meta["t"],
+                     fo=s.get("function_objects", []), region=rv)
+    for key, ref in arr.items():
+        assert bits_equal(out[key], ref), (key, rel_l2(out[key], ref))
+        assert np.all(rel_l2(out[key], ref) <= REF_TOL)
+
+
+@pytest.mark.parametrize("q", [19, 27])
+@pytest.mark.parametrize("tile", [(32, 8, None), (16, 8, None), (8, 8, None)])
+@pytest.mark.parametrize("z_chunk", [0, 8, 5])
+def test_tiling_and_chunking_do_not_change_results(q, tile, z_chunk):
+    """Every tile shape and z-chunk length computes the same bits."""
+    stages = 3 if q == 19 else 2
+    base = run_cavity(q, 32, 24, 40, 400.0, 0.05, 30, fo=("S", "kMean"), tile=(32, 8, stages))
+    out = run_cavity(q, 32, 24, 40, 400.0, 0.05, 30, fo=("S", "kMean"), tile=(tile[0], tile[1], stages),
+                     z_chunk=z_chunk)
+    for k in base:
+        assert bits_equal(out[k], base[k]), k
+
+
+@pytest.mark.parametrize("q", [19, 27])
+def test_against_fp64_oracle(q):
+    n = (24, 16, 32)
+    out = run_cavity(q, *n, 250.0, 0.05, 60, fo=("S", "SMean", "k", "kMean", "momentsMean"))
+    o = Oracle(q, *n, 250.0, 0.05)
+    m = o.initial(casefiles.scaled_region_values(casefiles.lid_cavity_values(0.05)))
+    fo = o.new_function_objects(["S", "SMean", "k", "kMean", "momentsMean"])
+    o.run(m, 60, 0, fo)
+    assert np.all(rel_l2(out["moments"], m) < 1e-3)
+    assert np.all(max_abs(out["moments"], m) < np.array([1e-5] + [2.5e-6] * 9))
+    for k in fo:
+        assert np.all(rel_l2(out[k], fo[k]) < 1e-3), k
+
+
+def test_fp64_means_agree_with_fp32_means():
+    a = run_cavity(19, 16, 16, 16, 100.0, 0.05, 40, fo=("SMean", "kMean", "momentsMean"))
+    c = Cavity(19, 16, 16, 16, 100.0, 0.05, function_objects=("SMean", "kMean", "momentsMean"), mean_bits=64)
+    c.init_regions()
+    c.step(40)
+    c.synchronize()
+    for k in ("SMean", "kMean", "momentsMean"):
+        d = c.read(k, dtype=np.float64)
+        assert np.all(rel_l2(d, a[k]) < 1e-5), k
+    c.close()
+
+
+@pytest.mark.parametrize("q", [19, 27])
+def test_restart_reproduces_continuous_run(q):
+    """N+M steps in one go == N steps, save (tiled .LBMBin order), restart, M steps."""
+    full = run_cavity(q, 16, 24, 16, 300.0, 0.05, 30)["moments"]
+    c = Cavity(q, 16, 24, 16, 300.0, 0.05)
+    c.init_regions()
+    c.step(18)
+    saved = c.read("moments", tiled=True)
+    c.close()
+    r = Cavity(q, 16, 24, 16, 300.0, 0.05, start_step=18)
+    r.write(saved, tiled=True)
+    r.step(12)
+    r.synchronize()
+    assert bits_equal(r.read("moments"), full)
+    assert r.info()["step"] == 30
+    r.close()
+
+
+def test_field_access_errors():
+    from cudalbm_b200._lib import LBMError
+
+    with Cavity(19, 16, 16, 16, 100.0, 0.05, function_objects=("k",)) as c:
+        c.init_regions()
+        with pytest.raises(LBMError) as e:
+            c.read("SMean")
+        assert e.value.status == 7
+        with pytest.raises(LBMError) as e:
+            c.write(np.zeros((3, 16, 16, 16), np.float32))
+        assert e.value.status == 1
+
+
+def test_reduction_and_large_mesh_properties():
+    """256^3 D3Q27 with all function objects: finite, mirror-symmetric in z to
+    FP32 rounding, mass conserved to the level the wet-node walls allow."""
+    n = 256
+    c = Cavity(27, n, n, n, 1000.0, 0.05, function_objects=("S", "SMean", "k", "kMean"))
+    c.init_regions()
+    r0 = c.reduce()
+    c.step(100)
+    c.synchronize()
+    r1 = c.reduce()
+    assert r1["nonfinite"] == 0
+    assert abs(r1["mass"] - r0["mass"]) / r0["mass"] < 1e-4
+    m = c.read("moments")
+    sign = np.array([1, 1, 1, -1, 1, 1, -1, 1, -1, 1], np.float32)[:, None, None]
+    scale = np.sqrt(np.mean(m.astype(np.float64) ** 2, axis=(1, 2, 3)))  # global RMS per field
+    # compare a few z-planes with their mirror images
+    for z in (0, 17, 100, 127):
+        a = m[:, z].astype(np.float64)
+        b = (sign * m[:, n - 1 - z]).astype(np.float64)
+        assert np.all(np.sqrt(np.mean((a - b) ** 2, axis=(1, 2))) / scale < 1e-4), z
+    c.close()
+
+
+# ------------------------------------------------------------ live reference
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+
+
+def have_ref(q):
+    return os.path.exists(os.path.join(REF_DIR, f"momentBasedD3Q{q}"))
+
+
+def ref_run(q, spec):
+    d = tempfile.mkdtemp()
+    casefiles.write_case(d, spec)
+    subprocess.run([os.path.join(REF_DIR, f"momentBasedD3Q{q}"), "-GPU", "0"], cwd=d, check=True,
+                   capture_output=True, timeout=900)
+    return d
+
+
+@pytest.mark.parametrize("q", [19, 27])
+def test_one_step_bitwise_against_live_reference(q):
+    if not have_ref(q):
+        pytest.skip("reference executables not built (make -f oracle/Makefile.ref)")
+    spec = casefiles.CaseSpec(nx=40, ny=24, nz=32, Re=200.0, u_inf=0.05, n_steps=12, save_interval=1,
+                              info_interval=100)
+    d = ref_run(q, spec)
+    for t in (0, 3, 10):
+        st = lbmbin.read(os.path.join(d, f"lidDrivenCavity_{t}.LBMBin")).data
+        nxt = lbmbin.read(os.path.join(d, f"lidDrivenCavity_{t + 1}.LBMBin")).data
+        c = Cavity(q, 40, 24, 32, 200.0, 0.05, start_step=t)
+        c.write(st)
+        c.step(1)
+        c.synchronize()
+        assert bits_equal(c.read("moments"), nxt), t
+        c.close()
+
+
+def test_config1_d3q19_64_re100_1000_steps_against_live_reference():
+    """The stated parity case: D3Q19 64^3, Re = 100, u_lid = 0.05, 1000 steps;
+    all 10 moments against the reference's own CUDA solver (relative L2 per
+    moment <= 1e-5; observed: bit-identical)."""
+    if not have_ref(19):
+        pytest.skip("reference executables not built (make -f oracle/Makefile.ref)")
+    spec = casefiles.CaseSpec(nx=64, ny=64, nz=64, Re=100.0, u_inf=0.05, n_steps=1001, save_interval=1000,
+                              info_interval=1000)
+    d = ref_run(19, spec)
+    ref = lbmbin.read(os.path.join(d, "lidDrivenCavity_1000.LBMBin")).data
+    out = run_cavity(19, 64, 64, 64, 100.0, 0.05, 1000)["moments"]
+    assert np.all(rel_l2(out, ref) <= REF_TOL)
+    assert bits_equal(out, ref)
