@@ -211,8 +211,9 @@ def run_ours(args, w):
 
     nx, ny, nz = w["n"]
     nodes = nx * ny * nz
+    tile = (args.tile_x, args.tile_y, args.stages) if args.tile_x else None
     cav = Cavity(w["lattice"], nx, ny, nz, w["Re"], w["u"], function_objects=w["fo"], mean_bits=w["mean_bits"],
-                 device=local)
+                 device=local, tile=tile, z_chunk=args.z_chunk)
     cav.init_regions()
     cav.step(args.warmup)
     cav.synchronize()
@@ -288,6 +289,7 @@ def run_ours(args, w):
         "gpu_launches": int(launches),
         "clocks": clocks,
         "check": {"mass": red["mass"], "nonfinite": red["nonfinite"]},
+        "kernel": {"tile": [info["tile_x"], info["tile_y"]], "z_chunk": info["z_chunk"], "stages": info["stages"]},
     }
     if world == 1 and not args.no_cpu_baseline:
         try:
@@ -371,6 +373,10 @@ def main():
     ap.add_argument("--workload", default="q27_256_fo", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tile-x", type=int, default=0, help="kernel tiling override (default: autotuned)")
+    ap.add_argument("--tile-y", type=int, default=8)
+    ap.add_argument("--stages", type=int, default=0)
+    ap.add_argument("--z-chunk", type=int, default=0)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -10,7 +10,9 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "liblbm_b200.so")
+# LBM_B200_LIBRARY selects another build of the same library (A/B timing of
+# kernel variants); the default is the in-tree build.
+LIB_PATH = os.environ.get("LBM_B200_LIBRARY") or os.path.join(HERE, "lib", "liblbm_b200.so")
 
 LBM_OK = 0
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4: "device wait timed out",

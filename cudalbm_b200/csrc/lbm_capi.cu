@@ -354,6 +354,12 @@ lbm_status launch_step(lbm_handle *h)
         p.fo.inv_count = 1.0f / static_cast<float>(h->t + 1);
     else
         p.fo.inv_count = 1.0 / static_cast<double>(h->t + 1);
+    // divisors 2*4.5*tau and 2*9*tau in float as the reference evaluates them;
+    // the host's float division is IEEE, so the reciprocals are RN(1/d)
+    p.fo.sd.d_ii = 2.0f * 4.5f * h->tau;
+    p.fo.sd.d_ij = 2.0f * 9.0f * h->tau;
+    p.fo.sd.r_ii = 1.0f / p.fo.sd.d_ii;
+    p.fo.sd.r_ij = 1.0f / p.fo.sd.d_ij;
     p.err = h->err;
     p.timeout_ns = 2000000000ull;
     const dim3 block(h->launcher.tx, h->launcher.ty);

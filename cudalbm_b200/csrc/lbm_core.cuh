@@ -75,9 +75,6 @@ __host__ __device__ constexpr int q_of_zslot(int c, int s)
     return -1;
 }
 
-template <int Q>
-__device__ __forceinline__ float weight_rho(float rho, int cls);
-
 struct Consts {
     static constexpr float cs2 = static_cast<float>(1.0 / 3.0);
 };
@@ -94,12 +91,6 @@ __host__ __device__ constexpr float weight(int cls)
                    : (cls == 0 ? static_cast<float>(8.0 / 27.0) : cls == 1 ? static_cast<float>(2.0 / 27.0)
                       : cls == 2 ? static_cast<float>(1.0 / 54.0) : static_cast<float>(1.0 / 216.0));
 }
-
-// Moments in registers: m[0] = rho (with the +1 offset applied), m[1..3] =
-// 3u, m[4,7,9] = 4.5 m_aa, m[5,6,8] = 9 m_ab (the reference's scaled units).
-struct Moments {
-    float m[10];
-};
 
 // ------------------------------------------------------ reconstruction
 // Bracketing per direction, as written in the reference:
@@ -196,34 +187,6 @@ __device__ __forceinline__ float fold_from(const float *f)
     }
 }
 
-// Masked variant for boundary nodes: directions that would stream in from
-// outside the domain contribute 0 (reference: incomingSwitch * f_q).
-__device__ __forceinline__ bool is_known(int q, unsigned type);
-
-template <int Q, int A, int B, int q>
-__device__ __forceinline__ float fold_masked(const float *f, const float *mask)
-{
-    if constexpr (q >= Q) {
-        return 0.0f;
-    } else {
-        constexpr int c = cdir(A, q) * cdir(B, q);
-        constexpr int nq = [] {
-            int r = q + 1;
-            while (r < Q && cdir(A, r) * cdir(B, r) == 0) r++;
-            return r;
-        }();
-        if constexpr (c == 0) {
-            return fold_masked<Q, A, B, nq>(f, mask);
-        } else {
-            const float e = (c > 0) ? mask[q] * f[q] : -mask[q] * f[q];
-            if constexpr (nq >= Q)
-                return e;
-            else
-                return e + fold_masked<Q, A, B, nq>(f, mask);
-        }
-    }
-}
-
 // node class bits (normalVector.cuh:321-334)
 enum : unsigned { WEST = 0x01, EAST = 0x02, SOUTH = 0x04, NORTH = 0x08, BACK = 0x10, FRONT = 0x20 };
 
@@ -233,55 +196,83 @@ __device__ __forceinline__ unsigned node_type(int x, int y, int z, int nx, int n
            (z == 0 ? BACK : 0u) | (z == nz - 1 ? FRONT : 0u);
 }
 
-// 1.0f if f_q is known at a node of this class, 0.0f if it streams in from
-// outside the domain.
-template <int q>
-__device__ __forceinline__ float known_switch(unsigned t)
+// Bit q set if direction q has the given sign along the given axis.
+template <int AXIS, int SIGN>
+__host__ __device__ constexpr unsigned dir_mask()
 {
-    constexpr int cx = cx_of(q), cy = cy_of(q), cz = cz_of(q);
-    const bool cond_x = ((t & EAST) && cx < 0) || ((t & WEST) && cx > 0);
-    const bool cond_y = ((t & NORTH) && cy < 0) || ((t & SOUTH) && cy > 0);
-    const bool cond_z = ((t & FRONT) && cz < 0) || ((t & BACK) && cz > 0);
-    return static_cast<float>(!(cond_x | cond_y | cond_z));
+    unsigned m = 0;
+    for (int q = 0; q < 27; q++) {
+        const int c = AXIS == 0 ? cx_of(q) : (AXIS == 1 ? cy_of(q) : cz_of(q));
+        if (c == SIGN)
+            m |= 1u << q;
+    }
+    return m;
 }
 
+// Directions that stream into a node of class t from outside the domain
+// (the complement of incomingSwitch, velocitySet.cuh:204-220).
+__device__ __forceinline__ unsigned unknown_dirs(unsigned t)
+{
+    return ((t & EAST) ? dir_mask<0, -1>() : 0u) | ((t & WEST) ? dir_mask<0, 1>() : 0u) |
+           ((t & NORTH) ? dir_mask<1, -1>() : 0u) | ((t & SOUTH) ? dir_mask<1, 1>() : 0u) |
+           ((t & FRONT) ? dir_mask<2, -1>() : 0u) | ((t & BACK) ? dir_mask<2, 1>() : 0u);
+}
+
+// The reference sums incomingSwitch*f_q with incomingSwitch in {0, 1}.  A zero
+// term leaves a right fold's value unchanged, so zeroing the unknown f_q and
+// folding as for an interior node gives the same bits as the masked sums.
 template <int Q, int q = 0>
-__device__ __forceinline__ void fill_mask(float *mask, unsigned t)
+__device__ __forceinline__ void zero_unknown(float *f, unsigned unknown)
 {
     if constexpr (q < Q) {
-        mask[q] = known_switch<q>(t);
-        fill_mask<Q, q + 1>(mask, t);
+        f[q] = ((unknown >> q) & 1u) ? 0.0f : f[q];
+        zero_unknown<Q, q + 1>(f, unknown);
     }
+}
+
+// The ten raw sums the moments are built from: sum f, sum f c_a, sum f c_a c_b.
+template <int Q>
+__device__ __forceinline__ void moment_folds(const float *f, float *s)
+{
+    s[0] = fold_from<Q, -1, -1, 0>(f);
+    s[1] = fold_from<Q, 0, -1, 0>(f);
+    s[2] = fold_from<Q, 1, -1, 0>(f);
+    s[3] = fold_from<Q, 2, -1, 0>(f);
+    s[4] = fold_from<Q, 0, 0, 0>(f);
+    s[5] = fold_from<Q, 0, 1, 0>(f);
+    s[6] = fold_from<Q, 0, 2, 0>(f);
+    s[7] = fold_from<Q, 1, 1, 0>(f);
+    s[8] = fold_from<Q, 1, 2, 0>(f);
+    s[9] = fold_from<Q, 2, 2, 0>(f);
 }
 
 struct Relax {
     float omega, t_omega, omega_d2, tau, u_lid;
 };
 
-// Interior moments (unscaled): velocitySet.cuh:398-417.
-template <int Q>
-__device__ __forceinline__ void interior_moments(const float *f, float *mom)
+// Interior moments (unscaled) from the folds: velocitySet.cuh:398-417.
+__device__ __forceinline__ void interior_moments(const float *s, float *mom)
 {
-    mom[0] = fold_from<Q, -1, -1, 0>(f);
+    mom[0] = s[0];
     const float inv_rho = 1.0f / mom[0];
-    mom[1] = fold_from<Q, 0, -1, 0>(f) * inv_rho;
-    mom[2] = fold_from<Q, 1, -1, 0>(f) * inv_rho;
-    mom[3] = fold_from<Q, 2, -1, 0>(f) * inv_rho;
-    mom[4] = (fold_from<Q, 0, 0, 0>(f) * inv_rho) - Consts::cs2;
-    mom[5] = fold_from<Q, 0, 1, 0>(f) * inv_rho;
-    mom[6] = fold_from<Q, 0, 2, 0>(f) * inv_rho;
-    mom[7] = (fold_from<Q, 1, 1, 0>(f) * inv_rho) - Consts::cs2;
-    mom[8] = fold_from<Q, 1, 2, 0>(f) * inv_rho;
-    mom[9] = (fold_from<Q, 2, 2, 0>(f) * inv_rho) - Consts::cs2;
+    mom[1] = s[1] * inv_rho;
+    mom[2] = s[2] * inv_rho;
+    mom[3] = s[3] * inv_rho;
+    mom[4] = (s[4] * inv_rho) - Consts::cs2;
+    mom[5] = s[5] * inv_rho;
+    mom[6] = s[6] * inv_rho;
+    mom[7] = (s[7] * inv_rho) - Consts::cs2;
+    mom[8] = s[8] * inv_rho;
+    mom[9] = (s[9] * inv_rho) - Consts::cs2;
 }
 
-// Wet-node boundary moments (unscaled), boundaryConditions.cuh:99-533.
+// Wet-node boundary moments (unscaled), boundaryConditions.cuh:99-533, from
+// the folds of the known populations (s[0] = rho_I, s[5,6,8] = the raw
+// c_a c_b sums whose quotients by rho_I are the reference's m_ab_I).
 template <int Q>
-__device__ __forceinline__ void boundary_moments(const float *f, unsigned t, const Relax &rx, float *mom)
+__device__ __forceinline__ void boundary_moments(const float *s, unsigned t, const Relax &rx, float *mom)
 {
-    float mask[Q];
-    fill_mask<Q>(mask, t);
-    const float rho_I = fold_masked<Q, -1, -1, 0>(f, mask);
+    const float rho_I = s[0];
     const float inv_rho_I = 1.0f / rho_I;
     const float omega = rx.omega;
     const float U = rx.u_lid;
@@ -297,9 +288,9 @@ __device__ __forceinline__ void boundary_moments(const float *f, unsigned t, con
     mom[7] = 0.0f;
     mom[9] = 0.0f;
 
-#define LBM_MXY_I (fold_masked<Q, 0, 1, 0>(f, mask) * inv_rho_I)
-#define LBM_MXZ_I (fold_masked<Q, 0, 2, 0>(f, mask) * inv_rho_I)
-#define LBM_MYZ_I (fold_masked<Q, 1, 2, 0>(f, mask) * inv_rho_I)
+#define LBM_MXY_I (s[5] * inv_rho_I)
+#define LBM_MXZ_I (s[6] * inv_rho_I)
+#define LBM_MYZ_I (s[8] * inv_rho_I)
     switch (t) {
     case SOUTH | WEST | BACK:
     case SOUTH | WEST | FRONT:
@@ -506,24 +497,118 @@ __device__ __forceinline__ void scale_collide(float *m, const Relax &rx)
 
 // Full node update from the streamed populations f[Q] (in direction order).
 // Returns the stored (post-collision) moments with rho still including rho0.
+// f is clobbered (unknown directions of boundary nodes are zeroed).
 template <int Q>
-__device__ __forceinline__ void node_update(const float *f, unsigned type, const Relax &rx, float *m)
+__device__ __forceinline__ void node_update(float *f, unsigned type, const Relax &rx, float *m)
 {
     if (type)
-        boundary_moments<Q>(f, type, rx, m);
+        zero_unknown<Q>(f, unknown_dirs(type));
+    float s[10];
+    moment_folds<Q>(f, s);
+    if (type)
+        boundary_moments<Q>(s, type, rx, m);
     else
-        interior_moments<Q>(f, m);
+        interior_moments(s, m);
     scale_collide(m, rx);
 }
 
 // ------------------------------------------------------- function objects
-__device__ __forceinline__ float strain_diag(float ua, float ub, float mab, float tau)
+// x / d rounded to nearest, for d > 0 and r = RN(1/d): q = RN(x r), the
+// remainder e = x - d q is exact by FMA, and RN(q + e r) is the correctly
+// rounded quotient (P. Markstein, "Computation of elementary functions on the
+// IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990) as long as
+// nothing underflows or overflows: numerators must lie in [2^-64, 2^64) in
+// magnitude (zeros excluded); div_unsafe(x) >= 128 flags the others, which
+// div_exact() handles.  Both are checked against IEEE division for every
+// float numerator by tests/cuda/div_exhaustive.cu.
+__device__ __forceinline__ float div_by_recip(float x, float d, float r)
 {
-    return 3.0f * ((ua * ub) - mab) / (2.0f * 4.5f * tau);
+    const float q = x * r;
+    const float e = fmaf(-d, q, x);
+    return fmaf(e, r, q);
 }
-__device__ __forceinline__ float strain_off(float ua, float ub, float mab, float tau)
+__device__ __forceinline__ unsigned div_unsafe(float x)
 {
-    return 3.0f * ((ua * ub) - mab) / (2.0f * 9.0f * tau);
+    return ((__float_as_uint(x) >> 23) & 0xffu) - 63u;  // >= 128 when outside the window
+}
+
+// x / d rounded to nearest-even for any float x and d in [1, 2^40) with
+// r = RN(1/d), using only multiplies and FMAs (no divide instruction):
+//  * zeros, infinities and NaN: x * r has the right value and sign;
+//  * |x| in [2^-64, 2^64): div_by_recip;
+//  * |x| >= 2^64: scale by 2^-96 (exact), divide, scale back (exact, or the
+//    same overflow to infinity as the IEEE quotient);
+//  * |x| < 2^-64 with a normal quotient: scale by 2^96, divide, scale back;
+//  * subnormal quotient: the result is n * 2^-149 with n = round-half-even of
+//    X / d, X = |x| * 2^149 (an integer-valued float below 2^23 d): q = RN(X/d)
+//    cannot cross a half-integer (those are representable), so rint(q) is n
+//    unless q is itself a half-integer, where the sign of the exact remainder
+//    X - d q decides.
+__device__ __forceinline__ float div_exact(float x, float d, float r)
+{
+    const unsigned ex = (__float_as_uint(x) >> 23) & 0xffu;
+    if (ex - 63u < 128u)
+        return div_by_recip(x, d, r);
+    if (x == 0.0f || ex == 0xffu)
+        return x * r;
+    const float ax = fabsf(x);
+    float y;
+    if (ex >= 191u) {
+        y = div_by_recip(ax * 0x1p-96f, d, r) * 0x1p96f;
+    } else {
+        const float ys = div_by_recip(ax * 0x1p96f, d, r);
+        if (ys >= 0x1p-30f) {
+            y = ys * 0x1p-96f;
+        } else {
+            const float X = ax * 0x1p100f * 0x1p49f;
+            const float q = div_by_recip(X, d, r);
+            const float fl = floorf(q);
+            float n = rintf(q);
+            if (q - fl == 0.5f) {
+                const float e = fmaf(-d, q, X);
+                n = e > 0.0f ? fl + 1.0f : (e < 0.0f ? fl : n);
+            }
+            y = n * 0x1p-100f * 0x1p-49f;
+        }
+    }
+    return copysignf(y, x);
+}
+
+// Divisors of the strain-rate tensor (strainRateTensor.cuh:71-90):
+// 2 * scale_ii * tau and 2 * scale_ij * tau, with their reciprocals.
+struct StrainDiv {
+    float d_ii, r_ii, d_ij, r_ij;
+};
+
+// S_ab = 3 (u_a u_b - m_ab) / (2 scale tau) for the six components
+// (xx, xy, xz, yy, yz, zz) of the stored moments m (u = m[1..3]).
+__device__ __forceinline__ void strain_rate(const float *m, const StrainDiv &sd, float *S)
+{
+    const float u = m[1], v = m[2], w = m[3];
+    float x[6];
+    x[0] = 3.0f * ((u * u) - m[4]);
+    x[1] = 3.0f * ((u * v) - m[5]);
+    x[2] = 3.0f * ((u * w) - m[6]);
+    x[3] = 3.0f * ((v * v) - m[7]);
+    x[4] = 3.0f * ((v * w) - m[8]);
+    x[5] = 3.0f * ((w * w) - m[9]);
+    const unsigned worst = max(max(max(div_unsafe(x[0]), div_unsafe(x[1])), max(div_unsafe(x[2]), div_unsafe(x[3]))),
+                               max(div_unsafe(x[4]), div_unsafe(x[5])));
+    if (worst < 128u) {
+        S[0] = div_by_recip(x[0], sd.d_ii, sd.r_ii);
+        S[1] = div_by_recip(x[1], sd.d_ij, sd.r_ij);
+        S[2] = div_by_recip(x[2], sd.d_ij, sd.r_ij);
+        S[3] = div_by_recip(x[3], sd.d_ii, sd.r_ii);
+        S[4] = div_by_recip(x[4], sd.d_ij, sd.r_ij);
+        S[5] = div_by_recip(x[5], sd.d_ii, sd.r_ii);
+    } else {
+        S[0] = div_exact(x[0], sd.d_ii, sd.r_ii);
+        S[1] = div_exact(x[1], sd.d_ij, sd.r_ij);
+        S[2] = div_exact(x[2], sd.d_ij, sd.r_ij);
+        S[3] = div_exact(x[3], sd.d_ii, sd.r_ii);
+        S[4] = div_exact(x[4], sd.d_ij, sd.r_ij);
+        S[5] = div_exact(x[5], sd.d_ii, sd.r_ii);
+    }
 }
 __device__ __forceinline__ float kinetic(float u, float v, float w)
 {

@@ -106,6 +106,7 @@ struct FOPtrs {
     MeanT *kMean;        // [N] or null
     MeanT *momentsMean;  // [10][N] or null
     MeanT inv_count;     // 1 / (t + 1), t the absolute step index
+    StrainDiv sd;        // divisors of S and their reciprocals
 };
 
 template <typename MeanT>
@@ -325,15 +326,9 @@ __global__ void __launch_bounds__(TX *TY) step_kernel(const __grid_constant__ CU
                 for (int k = 1; k < 10; k++)
                     o[k * N] = m[k];
                 if constexpr (FO) {
-                    const float u = m[1], v = m[2], w = m[3];
                     if (p.fo.S || p.fo.SMean) {
                         float s6[6];
-                        s6[0] = strain_diag(u, u, m[4], p.rx.tau);
-                        s6[1] = strain_off(u, v, m[5], p.rx.tau);
-                        s6[2] = strain_off(u, w, m[6], p.rx.tau);
-                        s6[3] = strain_diag(v, v, m[7], p.rx.tau);
-                        s6[4] = strain_off(v, w, m[8], p.rx.tau);
-                        s6[5] = strain_diag(w, w, m[9], p.rx.tau);
+                        strain_rate(m, p.fo.sd, s6);
                         if (p.fo.S) {
 #pragma unroll
                             for (int c = 0; c < 6; c++)
@@ -346,7 +341,7 @@ __global__ void __launch_bounds__(TX *TY) step_kernel(const __grid_constant__ CU
                         }
                     }
                     if (p.fo.k || p.fo.kMean) {
-                        const float ke = kinetic(u, v, w);
+                        const float ke = kinetic(m[1], m[2], m[3]);
                         if (p.fo.k)
                             p.fo.k[iu] = ke;
                         if (p.fo.kMean)

@@ -140,12 +140,13 @@ def test_reduction_and_large_mesh_properties():
     assert abs(r1["mass"] - r0["mass"]) / r0["mass"] < 1e-4
     m = c.read("moments")
     sign = np.array([1, 1, 1, -1, 1, 1, -1, 1, -1, 1], np.float32)[:, None, None]
-    scale = np.sqrt(np.mean(m.astype(np.float64) ** 2, axis=(1, 2, 3)))  # global RMS per field
-    # compare a few z-planes with their mirror images
+    # compare a few z-planes with their mirror images: the Back and Front
+    # formulas round differently, so the planes agree to FP32 rounding of the
+    # O(0.1) scaled moments, not bit for bit
     for z in (0, 17, 100, 127):
         a = m[:, z].astype(np.float64)
         b = (sign * m[:, n - 1 - z]).astype(np.float64)
-        assert np.all(np.sqrt(np.mean((a - b) ** 2, axis=(1, 2))) / scale < 1e-4), z
+        assert np.all(np.sqrt(np.mean((a - b) ** 2, axis=(1, 2))) < 2e-6), z
     c.close()
 
 
