@@ -29,7 +29,8 @@ F32, F64 = 0, 1
 # every symbol include/lbm_b200.h declares
 EXPORTS = ("lbm_config_default", "lbm_create", "lbm_destroy", "lbm_init_regions", "lbm_write_fields",
            "lbm_read_fields", "lbm_step", "lbm_synchronize", "lbm_reduce", "lbm_get_info", "lbm_last_error",
-           "lbm_status_string", "lbm_field_set_vars", "lbm_host_alloc", "lbm_host_free")
+           "lbm_status_string", "lbm_field_set_vars", "lbm_host_alloc", "lbm_host_free", "lbm_case_read",
+           "lbm_lbmbin_write")
 
 
 class Config(ctypes.Structure):
@@ -45,6 +46,15 @@ class Info(ctypes.Structure):
                 ("omega", ctypes.c_float), ("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32),
                 ("z_chunk", ctypes.c_int32), ("stages", ctypes.c_int32), ("device_bytes", ctypes.c_uint64),
                 ("last_step_ms", ctypes.c_double), ("kernel_launches", ctypes.c_uint64)]
+
+
+class Case(ctypes.Structure):
+    _fields_ = [("case_name", ctypes.c_char * 256), ("Re", ctypes.c_float), ("u_inf", ctypes.c_float),
+                ("n_time_steps", ctypes.c_uint64), ("save_interval", ctypes.c_uint64),
+                ("info_interval", ctypes.c_uint64), ("nx", ctypes.c_uint64), ("ny", ctypes.c_uint64),
+                ("nz", ctypes.c_uint64), ("Lx", ctypes.c_float), ("Ly", ctypes.c_float), ("Lz", ctypes.c_float),
+                ("function_objects", ctypes.c_uint32), ("region", ctypes.c_float * 70),
+                ("latest_time", ctypes.c_uint64), ("has_restart", ctypes.c_int32)]
 
 
 class LBMError(RuntimeError):
@@ -81,8 +91,12 @@ def lib() -> ctypes.CDLL:
         L.lbm_field_set_vars.argtypes = [i32]
         L.lbm_host_alloc.argtypes = [sz, ctypes.POINTER(vp)]
         L.lbm_host_free.argtypes = [vp]
+        L.lbm_case_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(Case)]
+        L.lbm_lbmbin_write.argtypes = [ctypes.c_char_p, u64, u64, u64, i32, ctypes.POINTER(ctypes.c_char_p), vp, u64,
+                                       i32]
         for name in ("lbm_create", "lbm_destroy", "lbm_init_regions", "lbm_write_fields", "lbm_read_fields",
-                     "lbm_step", "lbm_synchronize", "lbm_reduce", "lbm_get_info", "lbm_host_alloc", "lbm_host_free"):
+                     "lbm_step", "lbm_synchronize", "lbm_reduce", "lbm_get_info", "lbm_host_alloc", "lbm_host_free",
+                     "lbm_case_read", "lbm_lbmbin_write"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -118,3 +132,15 @@ class PinnedArray:
             self.free()
         except Exception:
             pass
+
+
+def read_case(directory: str) -> dict:
+    """Parse a case directory with the library's reader (lbm_case_read)."""
+    import numpy as np
+
+    c = Case()
+    check(lib().lbm_case_read(directory.encode(), ctypes.byref(c)))
+    out = {f: getattr(c, f) for f, _ in Case._fields_ if f not in ("case_name", "region")}
+    out["case_name"] = c.case_name.decode()
+    out["region"] = np.ctypeslib.as_array(c.region).reshape(10, 7).copy()
+    return out

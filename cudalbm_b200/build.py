@@ -27,8 +27,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-cudart", "static",
               "-I" + INCLUDE, "-I" + CSRC] + ARCH
 
-LIB_SOURCES = ["lbm_capi.cu"]
-HOST_SOURCES = ["casefile.cpp", "lbmbin.cpp"]
+LIB_SOURCES = ["lbm_capi.cu", "casefile.cpp", "lbmbin.cpp"]
 
 
 def _nvcc() -> str:
@@ -66,18 +65,25 @@ def build_library(force: bool = False, verbose_ptxas: bool = False) -> str:
     return LIB
 
 
+def _cxx() -> str:
+    # the system compiler (a g++ earlier on PATH may lack parts of libstdc++)
+    for cand in ("/usr/bin/g++", shutil.which("g++")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("g++ not found")
+
+
 def build_executables(force: bool = False) -> list:
+    """momentBasedD3Q19 / momentBasedD3Q27: host C++ over the library."""
     out = []
     main = os.path.join(CSRC, "solver_main.cpp")
-    if not os.path.exists(main):
-        return out
     os.makedirs(BIN, exist_ok=True)
-    host = [os.path.join(CSRC, s) for s in HOST_SOURCES if os.path.exists(os.path.join(CSRC, s))]
+    host = [os.path.join(CSRC, s) for s in ("casefile.cpp", "lbmbin.cpp")]
     for q in (19, 27):
         exe = os.path.join(BIN, f"momentBasedD3Q{q}")
         if force or _stale(exe, _deps() + [LIB]):
-            _run([_nvcc(), "-std=c++17", "-O2", "-I" + INCLUDE, "-I" + CSRC, f"-DLBM_LATTICE={q}", main] + host +
-                 ["-o", exe, "-L" + os.path.dirname(LIB), "-llbm_b200", "-Xlinker", "-rpath=$ORIGIN/../lib"])
+            _run([_cxx(), "-std=c++17", "-O2", "-Wall", "-I" + INCLUDE, "-I" + CSRC, f"-DLBM_LATTICE={q}", main] + host +
+                 ["-o", exe, "-L" + os.path.dirname(LIB), "-llbm_b200", "-Wl,-rpath,$ORIGIN/../lib"])
         out.append(exe)
     return out
 

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -18,8 +19,10 @@
 #include <utility>
 #include <vector>
 
+#include "casefile.hpp"
 #include "lbm_b200.h"
 #include "lbm_step.cuh"
+#include "lbmbin.hpp"
 
 namespace {
 
@@ -694,6 +697,58 @@ lbm_status lbm_reduce(lbm_handle *h, double out[3])
     out[0] = r[0];
     out[1] = r[1];
     out[2] = double(bad);
+    return LBM_OK;
+}
+
+lbm_status lbm_case_read(const char *dir, lbm_case *out)
+{
+    if (!dir || !out)
+        return fail(LBM_ERR_ARG, "null argument");
+    std::memset(out, 0, sizeof(*out));
+    try {
+        const lbm::ProgramControl pc = lbm::read_program_control(dir);
+        if (pc.caseName.size() >= sizeof(out->case_name))
+            return fail(LBM_ERR_PARSE, "caseName too long");
+        std::strncpy(out->case_name, pc.caseName.c_str(), sizeof(out->case_name) - 1);
+        out->Re = pc.Re;
+        out->u_inf = pc.u_inf;
+        out->n_time_steps = pc.nTimeSteps;
+        out->save_interval = pc.saveInterval;
+        out->info_interval = pc.infoInterval;
+        const lbm::LatticeMesh m = lbm::read_lattice_mesh(dir);
+        out->nx = m.nx;
+        out->ny = m.ny;
+        out->nz = m.nz;
+        out->Lx = m.Lx;
+        out->Ly = m.Ly;
+        out->Lz = m.Lz;
+        out->function_objects = lbm::read_function_objects(dir);
+        const std::vector<uint64_t> t = lbm::time_indices(dir, pc.caseName);
+        out->has_restart = !t.empty();
+        out->latest_time = t.empty() ? 0 : t.back();
+        if (t.empty()) {
+            const std::array<float, 70> r = lbm::read_initial_conditions(dir);
+            std::copy(r.begin(), r.end(), out->region);
+        }
+    } catch (const lbm::CaseError &e) {
+        return fail(std::string(e.what()).find("not opened") != std::string::npos ? LBM_ERR_IO : LBM_ERR_PARSE, e.what());
+    } catch (const std::exception &e) {
+        return fail(LBM_ERR_PARSE, e.what());
+    }
+    return LBM_OK;
+}
+
+lbm_status lbm_lbmbin_write(const char *path, uint64_t nx, uint64_t ny, uint64_t nz, int32_t nvars,
+                            const char *const *names, const float *values, uint64_t time_step, int32_t time_average)
+{
+    if (!path || !names || !values || nvars <= 0)
+        return fail(LBM_ERR_ARG, "null or empty argument");
+    try {
+        std::vector<std::string> n(names, names + nvars);
+        lbm::write_field_file(path, nx, ny, nz, n, values, time_step, time_average != 0);
+    } catch (const std::exception &e) {
+        return fail(LBM_ERR_IO, e.what());
+    }
     return LBM_OK;
 }
 

@@ -1,0 +1,269 @@
+// solver_main.cpp -- the momentBasedD3Q19 / momentBasedD3Q27 executables.
+//
+// Drop-in replacements for the reference's applications/momentBasedD3Q19 and
+// momentBasedD3Q27 (momentBasedD3Q19.cu:56-140): run inside a case directory
+// with `momentBasedD3Q19 -GPU <id>`, read programControl, latticeMesh,
+// initialConditions and functionObjects, restart from the latest
+// <caseName>_<t>.LBMBin if there is one, and write the same .LBMBin files at
+// the same steps.  The lattice is fixed at compile time (LBM_LATTICE).
+//
+// The time loop keeps the reference's order -- at step t: print if
+// t % infoInterval == 0, save if t % saveInterval == 0, then advance -- but
+// queues the steps between two such events without synchronising the device.
+//
+// Optional file b200Options (ignored by the reference) may set
+// `meanPrecision 64;` for double-precision running means.
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <limits>
+#include <sstream>
+#include <cstdio>
+#include <ctime>
+#include <filesystem>
+#include <iomanip>
+#include <iostream>
+#include <string>
+#include <vector>
+
+#include "casefile.hpp"
+#include "lbm_b200.h"
+#include "lbmbin.hpp"
+
+#ifndef LBM_LATTICE
+#define LBM_LATTICE 19
+#endif
+
+namespace {
+
+struct Failure {
+    int code;
+    std::string msg;
+};
+
+void check(lbm_status s)
+{
+    if (s != LBM_OK)
+        throw Failure{int(s), std::string(lbm_status_string(s)) + ": " + lbm_last_error()};
+}
+
+std::vector<int> parse_gpu_list(int argc, char **argv)
+{
+    const std::string exe = std::filesystem::path(argv[0]).filename().string();
+    for (int i = 1; i < argc; i++) {
+        if (std::string(argv[i]) != "-GPU")
+            continue;
+        if (i + 1 >= argc)
+            throw lbm::CaseError("Input argument -GPU has not been supplied with a value; the correct syntax is -GPU 0,1 for example");
+        std::vector<int> ids;
+        std::string s = argv[i + 1], cur;
+        for (char c : s + ",") {
+            if (c == ',') {
+                if (!cur.empty()) {
+                    if (!lbm::is_number(cur) || cur.find('.') != std::string::npos)
+                        throw lbm::CaseError("-GPU is not numeric");
+                    ids.push_back(std::stoi(cur));
+                }
+                cur.clear();
+            } else {
+                cur.push_back(c);
+            }
+        }
+        if (ids.empty())
+            throw lbm::CaseError("-GPU is not numeric");
+        return ids;
+    }
+    throw lbm::CaseError("Error: The -GPU argument is mandatory for the " + exe + " executable.");
+}
+
+void print_velocity_set()
+{
+    static const int cx[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1};
+    static const int cy[27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1, 1, -1};
+    static const int cz[27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, -1, 1, -1, 1, 1, -1, -1, 1, 1, -1, 1, -1};
+    const int Q = LBM_LATTICE;
+    std::cout << "D3Q" << Q << " {w, cx, cy, cz}:\n{\n";
+    for (int q = 0; q < Q; q++) {
+        const int n = (cx[q] != 0) + (cy[q] != 0) + (cz[q] != 0);
+        const double w = Q == 19 ? (n == 0 ? 1.0 / 3 : n == 1 ? 1.0 / 18 : 1.0 / 36)
+                                 : (n == 0 ? 8.0 / 27 : n == 1 ? 2.0 / 27 : n == 2 ? 1.0 / 54 : 1.0 / 216);
+        std::cout << "    [" << q << "] = {" << w << ", " << cx[q] << ", " << cy[q] << ", " << cz[q] << "};\n";
+    }
+    std::cout << "};\n" << std::endl;
+}
+
+const std::vector<std::string> kMoments = {"rho", "u", "v", "w", "m_xx", "m_xy", "m_xz", "m_yy", "m_yz", "m_zz"};
+
+std::vector<std::string> with_suffix(std::vector<std::string> v, const std::string &s)
+{
+    for (auto &x : v)
+        x += s;
+    return v;
+}
+
+struct Saver {
+    lbm_handle *h;
+    const lbm::LatticeMesh &mesh;
+    uint64_t N;
+    uint32_t fo;
+    int mean_bits;
+
+    void field(lbm_field_set set, const std::string &prefix, const std::vector<std::string> &names, uint64_t t,
+               bool mean) const
+    {
+        const size_t count = names.size() * N;
+        const std::string path = prefix + "_" + std::to_string(t) + ".LBMBin";
+        if (mean && mean_bits == 64) {
+            std::vector<double> buf(count);
+            check(lbm_read_fields(h, set, buf.data(), count, LBM_F64, LBM_ORDER_TILED));
+            lbm::write_field_file(path, mesh.nx, mesh.ny, mesh.nz, names, buf.data(), t, true);
+        } else {
+            std::vector<float> buf(count);
+            check(lbm_read_fields(h, set, buf.data(), count, LBM_F32, LBM_ORDER_TILED));
+            lbm::write_field_file(path, mesh.nx, mesh.ny, mesh.nz, names, buf.data(), t, mean);
+        }
+    }
+
+    // the case file and then the function objects, in the reference's order
+    // (objectRegistry.cuh:150-198: momentsMean, S, SMean, k, kMean)
+    void all(const std::string &caseName, uint64_t t) const
+    {
+        field(LBM_FIELDS_MOMENTS, caseName, kMoments, t, false);
+        const std::vector<std::string> S = {"S_xx", "S_xy", "S_xz", "S_yy", "S_yz", "S_zz"};
+        if (fo & LBM_FO_MOMENTSMEAN)
+            field(LBM_FIELDS_MOMENTSMEAN, "momentsMean", with_suffix(kMoments, "Mean"), t, true);
+        if (fo & LBM_FO_S)
+            field(LBM_FIELDS_S, "S", S, t, false);
+        if (fo & LBM_FO_SMEAN)
+            field(LBM_FIELDS_SMEAN, "SMean", with_suffix(S, "Mean"), t, true);
+        if (fo & LBM_FO_K)
+            field(LBM_FIELDS_K, "k", {"k"}, t, false);
+        if (fo & LBM_FO_KMEAN)
+            field(LBM_FIELDS_KMEAN, "kMean", {"kMean"}, t, true);
+    }
+};
+
+std::string hms(long long s)
+{
+    std::ostringstream o;
+    o << s / 3600 << ":" << std::setfill('0') << std::setw(2) << (s % 3600) / 60 << ":" << std::setfill('0')
+      << std::setw(2) << s % 60;
+    return o.str();
+}
+
+int run(int argc, char **argv)
+{
+    const std::vector<int> gpus = parse_gpu_list(argc, argv);
+    const lbm::ProgramControl pc = lbm::read_program_control(".");
+    const std::vector<uint64_t> times = lbm::time_indices(".", pc.caseName);
+    const uint64_t latest = times.empty() ? 0 : times.back();
+
+    const std::time_t now = std::time(nullptr);
+    std::cout << "programControl:\n{\n"
+              << "    programName: " << argv[0] << ";\n"
+              << "    launchTime: " << std::put_time(std::localtime(&now), "%Y-%m-%d %H:%M:%S") << ";\n"
+              << "    launchDirectory: " << std::filesystem::current_path().string() << ";\n"
+              << "    deviceList: [";
+    for (size_t i = 0; i < gpus.size(); i++)
+        std::cout << gpus[i] << (i + 1 < gpus.size() ? ", " : "");
+    std::cout << "];\n    caseName: " << pc.caseName << ";\n    Re = " << pc.Re << ";\n    nTimeSteps = " << pc.nTimeSteps
+              << ";\n    saveInterval = " << pc.saveInterval << ";\n    infoInterval = " << pc.infoInterval
+              << ";\n    latestTime = " << latest << ";\n    scalarType: 32 bit;\n    labelType: uint64_t;\n};\n"
+              << std::endl;
+
+    const lbm::LatticeMesh mesh = lbm::read_lattice_mesh(".");
+    std::cout << "latticeMesh:\n{\n    nx = " << mesh.nx << ";\n    ny = " << mesh.ny << ";\n    nz = " << mesh.nz
+              << ";\n    Lx = " << mesh.Lx << ";\n    Ly = " << mesh.Ly << ";\n    Lz = " << mesh.Lz << ";\n};\n"
+              << std::endl;
+    if (mesh.nx % 8 || mesh.ny % 8 || mesh.nz % 8 || !mesh.nx || !mesh.ny || !mesh.nz)
+        throw lbm::CaseError("block::nx() * mesh.nxBlocks() not equal to mesh.nx()\nMesh dimensions should be multiples of 8");
+    print_velocity_set();
+
+    lbm_config cfg;
+    lbm_config_default(&cfg);
+    cfg.lattice = LBM_LATTICE;
+    cfg.device = gpus[0];
+    cfg.nx = int64_t(mesh.nx);
+    cfg.ny = int64_t(mesh.ny);
+    cfg.nz = int64_t(mesh.nz);
+    cfg.Re = pc.Re;
+    cfg.u_inf = pc.u_inf;
+    cfg.function_objects = lbm::read_function_objects(".");
+    cfg.start_step = int64_t(latest);
+    if (std::filesystem::exists("b200Options")) {
+        const lbm::Lines L = lbm::read_lines("b200Options");
+        try {
+            cfg.mean_bits = std::stoi(lbm::parameter_string(L, "meanPrecision"));
+        } catch (const lbm::CaseError &) {
+        }
+    }
+    lbm_handle *h = nullptr;
+    check(lbm_create(&cfg, &h));
+    const uint64_t N = mesh.nx * mesh.ny * mesh.nz;
+
+    if (!times.empty()) {
+        // restart: every moment from the latest file, by name (hostArray.cuh:264-276)
+        const std::string file = pc.caseName + "_" + std::to_string(latest) + ".LBMBin";
+        std::vector<float> all(10 * N);
+        for (int f = 0; f < 10; f++) {
+            const std::vector<float> v = lbm::read_field_by_name(file, kMoments[f]);
+            if (v.size() != N)
+                throw lbm::CaseError("Field size mismatch in " + file);
+            std::copy(v.begin(), v.end(), all.begin() + f * N);
+        }
+        // running means restart from zero, as in the reference (their count keeps the absolute step)
+        check(lbm_write_fields(h, LBM_FIELDS_MOMENTS, all.data(), all.size(), LBM_F32, LBM_ORDER_TILED));
+    } else {
+        const std::array<float, 70> region = lbm::read_initial_conditions(".");
+        check(lbm_init_regions(h, region.data()));
+    }
+
+    const Saver save{h, mesh, N, cfg.function_objects, cfg.mean_bits};
+    std::cout << "Time loop start\n" << std::endl;
+    const auto start = std::chrono::high_resolution_clock::now();
+    uint64_t t = latest;
+    while (t < pc.nTimeSteps) {
+        if (t % pc.infoInterval == 0) {
+            check(lbm_synchronize(h));
+            std::cout << "Time: " << t << std::endl;
+        }
+        if (t % pc.saveInterval == 0)
+            save.all(pc.caseName, t);
+        // advance to the next step that prints or saves
+        uint64_t next = std::min(pc.nTimeSteps, std::min((t / pc.infoInterval + 1) * pc.infoInterval,
+                                                         (t / pc.saveInterval + 1) * pc.saveInterval));
+        check(lbm_step(h, next - t));
+        t = next;
+    }
+    check(lbm_synchronize(h));
+    const auto end = std::chrono::high_resolution_clock::now();
+    const long long secs = std::chrono::duration_cast<std::chrono::seconds>(end - start).count();
+    const double wall = std::chrono::duration<double>(end - start).count();
+    const uint64_t nsteps = pc.nTimeSteps > latest ? pc.nTimeSteps - latest : 0;
+    std::cout << "\nElapsed time: " << hms(secs) << "\n" << std::endl;
+    // the reference's figure: integer seconds, nt - latestTime - 1 steps (runTimeIO.cuh:144-165)
+    const double ref_mlups = secs > 0 ? double(N) * double(nsteps > 0 ? nsteps - 1 : 0) / (1e6 * double(secs))
+                                      : std::numeric_limits<double>::infinity();
+    std::cout << "MLUPS: " << ref_mlups << "\n" << std::endl;
+    std::cout << "MLUPS (wall clock, " << nsteps << " steps incl. IO): " << (wall > 0 ? double(N) * nsteps / wall / 1e6 : 0)
+              << "\n" << std::endl;
+    std::cout << "End\n" << std::endl;
+    lbm_destroy(h);
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char **argv)
+{
+    try {
+        return run(argc, argv);
+    } catch (const Failure &f) {
+        std::cerr << f.msg << std::endl;
+        return f.code;
+    } catch (const std::exception &e) {
+        std::cerr << "terminate called after throwing an instance of 'std::runtime_error'\n  what():  " << e.what()
+                  << std::endl;
+        return 134;
+    }
+}

@@ -146,6 +146,36 @@ lbm_status lbm_get_info(lbm_handle *h, lbm_info *info);
 lbm_status lbm_host_alloc(size_t bytes, void **out);
 lbm_status lbm_host_free(void *p);
 
+/* ------------------------------------------------------------------ case IO */
+
+/* A case directory as the reference solvers read it. */
+typedef struct lbm_case {
+    char case_name[256];
+    float Re, u_inf;                 /* programControl */
+    uint64_t n_time_steps, save_interval, info_interval;
+    uint64_t nx, ny, nz;             /* latticeMesh */
+    float Lx, Ly, Lz;
+    uint32_t function_objects;       /* functionObjects -> LBM_FO_* mask */
+    float region[70];                /* initialConditions, scaled as for lbm_init_regions */
+    uint64_t latest_time;            /* largest t of <case_name>_<t>.LBMBin in the directory */
+    int32_t has_restart;             /* 1 if such a file exists */
+} lbm_case;
+
+/* Parse the case files in `dir`.  Replaces programControl
+ * (src/programControl/programControl.cuh:69-124), host::latticeMesh parsing
+ * (src/latticeMesh/latticeMesh.cuh:85-131), boundaryValue/boundaryFields
+ * (src/boundaryConditions/boundaryValue.cuh:147-254), initialiserSwitch
+ * (src/functionObjects/functionObjects.cuh:104-107) and fileIO::latestTime
+ * (src/fileIO/fileIO.cuh:222-233).  The initial conditions are read only if
+ * there is no restart file, as in the reference. */
+lbm_status lbm_case_read(const char *dir, lbm_case *out);
+
+/* Write an .LBMBin file (fileIO::writeFile, src/fileIO/fileOutput.cuh:82-183):
+ * `values` holds nvars*nx*ny*nz floats in [field][block-tiled node] order. */
+lbm_status lbm_lbmbin_write(const char *path, uint64_t nx, uint64_t ny, uint64_t nz, int32_t nvars,
+                            const char *const *names, const float *values, uint64_t time_step,
+                            int32_t time_average);
+
 /* Message of the last failure on this thread (empty if none). */
 const char *lbm_last_error(void);
 

@@ -1,0 +1,77 @@
+"""The momentBasedD3Q19 / momentBasedD3Q27 executables as drop-in
+replacements: same case directory, same command line, and every .LBMBin file
+identical byte for byte to what the reference executables write."""
+import os
+import shutil
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from cudalbm_b200 import casefiles, lbmbin
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BIN = os.path.join(ROOT, "cudalbm_b200", "bin")
+REF = os.path.join(ROOT, "oracle", "_ref")
+
+
+def run(exe, case, check=True):
+    return subprocess.run([exe, "-GPU", "0"], cwd=case, capture_output=True, text=True, timeout=600, check=check)
+
+
+def lbmbin_files(d):
+    return sorted(f for f in os.listdir(d) if f.endswith(".LBMBin"))
+
+
+@pytest.mark.parametrize("q", [19, 27])
+def test_outputs_identical_to_reference_executable(q):
+    if not os.path.exists(os.path.join(REF, f"momentBasedD3Q{q}")):
+        pytest.skip("reference executables not built")
+    spec = casefiles.CaseSpec(nx=32, ny=24, nz=16, Re=300.0, u_inf=0.05, n_steps=61, save_interval=20,
+                              info_interval=10, function_objects=("S", "SMean", "k", "kMean", "momentsMean"))
+    ours, ref = tempfile.mkdtemp(), tempfile.mkdtemp()
+    casefiles.write_case(ours, spec)
+    casefiles.write_case(ref, spec)
+    out = run(os.path.join(BIN, f"momentBasedD3Q{q}"), ours)
+    run(os.path.join(REF, f"momentBasedD3Q{q}"), ref)
+    files = lbmbin_files(ref)
+    assert len(files) == 4 * 6 and lbmbin_files(ours) == files
+    for f in files:
+        a = open(os.path.join(ours, f), "rb").read()
+        b = open(os.path.join(ref, f), "rb").read()
+        assert a == b, f
+    assert "Time: 60" in out.stdout and "MLUPS" in out.stdout
+
+
+def test_restart_continues_like_one_run():
+    spec = casefiles.CaseSpec(nx=16, ny=16, nz=24, Re=200.0, u_inf=0.05, n_steps=41, save_interval=20,
+                              info_interval=20)
+    one, two = tempfile.mkdtemp(), tempfile.mkdtemp()
+    casefiles.write_case(one, spec)
+    casefiles.write_case(two, casefiles.CaseSpec(**{**spec.__dict__, "n_steps": 21}))
+    exe = os.path.join(BIN, "momentBasedD3Q19")
+    run(exe, one)
+    run(exe, two)
+    casefiles.write_case(two, spec)  # extend nTimeSteps, keep lidDrivenCavity_20.LBMBin
+    out = run(exe, two)
+    assert "latestTime = 20" in out.stdout
+    a = lbmbin.read(os.path.join(one, "lidDrivenCavity_40.LBMBin")).data
+    b = lbmbin.read(os.path.join(two, "lidDrivenCavity_40.LBMBin")).data
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_command_line_and_case_errors():
+    exe = os.path.join(BIN, "momentBasedD3Q19")
+    d = tempfile.mkdtemp()
+    casefiles.write_case(d, casefiles.CaseSpec(nx=12, ny=16, nz=16, Re=100.0, u_inf=0.05, n_steps=2,
+                                               save_interval=1, info_interval=1))
+    r = subprocess.run([exe], cwd=d, capture_output=True, text=True)
+    assert r.returncode != 0 and "-GPU argument is mandatory" in r.stderr
+    r = run(exe, d, check=False)
+    assert r.returncode != 0 and "multiples of 8" in r.stderr
+    os.remove(os.path.join(d, "latticeMesh"))
+    r = run(exe, d, check=False)
+    assert r.returncode != 0 and "latticeMesh file not opened" in r.stderr
