@@ -27,7 +27,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-cudart", "static",
               "-I" + INCLUDE, "-I" + CSRC] + ARCH
 
-LIB_SOURCES = ["lbm_capi.cu", "casefile.cpp", "lbmbin.cpp"]
+LIB_SOURCES = ["lbm_capi.cu", "lbm_noalloc.cu", "casefile.cpp", "lbmbin.cpp"]
 
 
 def _nvcc() -> str:

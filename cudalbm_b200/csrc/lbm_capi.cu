@@ -379,6 +379,14 @@ lbm_status launch_step(lbm_handle *h)
 
 }  // namespace
 
+namespace lbm {
+// Lets other translation units of the library report through lbm_last_error().
+lbm_status record_error(lbm_status s, const std::string &msg)
+{
+    return fail(s, msg);
+}
+}  // namespace lbm
+
 extern "C" {
 
 void lbm_config_default(lbm_config *c)

@@ -140,6 +140,21 @@ lbm_status lbm_reduce(lbm_handle *h, double out[3]);
 
 lbm_status lbm_get_info(lbm_handle *h, lbm_info *info);
 
+/* The sums of lbm_reduce over a caller-owned device array of moments
+ * ([10][nodes] floats in the stored units, on the calling thread's current
+ * device), for callers that must not allocate device memory: frameworks whose
+ * caching allocator owns all device memory, monitors of buffers they do not
+ * own, code without an lbm_handle.  It allocates nothing: its scratch (one
+ * partial sum per 16384 nodes) is a fixed 1.5 MiB device array of the library,
+ * present on every GPU that loads it, so at most 2^30 nodes are accepted
+ * (LBM_ERR_ARG beyond).  Sums use a fixed order, so repeated calls agree bit
+ * for bit.  The first call on a device looks up the array's address; make it
+ * before any stream capture.  Calls share the array: calls that overlap on the
+ * GPU race and must be serialised.  `stream` is a cudaStream_t (NULL: default
+ * stream); the call returns after the result is on the host.
+ * No counterpart in the reference, which has no allocation-free entry point. */
+lbm_status lbm_reduce_moments_noalloc(const float *moments, uint64_t nodes, double out[3], void *stream);
+
 /* Page-locked host memory for fast transfers (cudaMallocHost); free with
  * lbm_host_free.  Replaces: the reference's pinned host::array variant
  * (src/array/hostArray.cuh:66-140). */
