@@ -12,9 +12,10 @@ time step of the whole cavity.  Prints one JSON line (rank 0).
               stream, inputs resident in HBM; the moment buffers, 1.3 GB, are
               far larger than the 126 MB L2, so no flush is needed).
 * e2e         the same metric through the C ABI with host buffers: upload of
-              the state from pinned host memory, K x (lbm_step + lbm_reduce,
-              whose 24-byte result is read back every step), download of the
-              moments and function objects -- all inside the timed region.
+              the state from pinned host memory, K x lbm_step_monitored (each
+              step's 24-byte FP64 sums -- mass, kinetic energy, non-finite
+              count -- copied back to pinned memory), download of the moments
+              and function objects -- all inside the timed region.
 * roofline    algorithmic bytes per node update (reference tiling: 134 B for
               D3Q27 + 4 + 24 + 48 + 8 B for k, S, SMean, kMean = 218 B) times
               the nodes per launch over the measured launch time, against the
@@ -62,6 +63,11 @@ WORKLOADS = {
                     desc="D3Q27 lid-driven cavity 256^3, Re=1000, u_lid=0.05"),
     "q19_512": dict(lattice=19, n=(512, 512, 512), Re=1000.0, u=0.05, fo=(), mean_bits=32, b_alg=110,
                     desc="D3Q19 lid-driven cavity 512^3, Re=1000, u_lid=0.05"),
+    "q27_128_fo": dict(lattice=27, n=(128, 128, 128), Re=1000.0, u=0.05, fo=("S", "SMean", "k", "kMean"),
+                       mean_bits=32, b_alg=218,
+                       desc="D3Q27 lid-driven cavity 128^3, Re=1000, function objects S/SMean/k/kMean (profiling size)"),
+    "q19_128": dict(lattice=19, n=(128, 128, 128), Re=1000.0, u=0.05, fo=(), mean_bits=32, b_alg=110,
+                    desc="D3Q19 lid-driven cavity 128^3, Re=1000 (profiling size)"),
     "q27_256_fo64": dict(lattice=27, n=(256, 256, 256), Re=1000.0, u=0.05, fo=("S", "SMean", "k", "kMean"),
                          mean_bits=64, b_alg=274,
                          desc="D3Q27 lid-driven cavity 256^3, Re=1000, function objects with FP64 means"),
@@ -239,13 +245,13 @@ def run_ours(args, w):
     cav.read("moments", out=state.array)
     outs = {fs: _lib.PinnedArray((NVARS[fs], nz, ny, nx), np.float64 if (w["mean_bits"] == 64 and "Mean" in fs)
                                  else np.float32) for fs in ("moments",) + tuple(w["fo"])}
+    mon = _lib.PinnedArray((args.steps,), np.dtype(_lib.MONITOR_DTYPE))
     barrier()
     cav.synchronize()
     t0 = time.perf_counter()
     cav.write(state.array)
-    for _ in range(args.steps):
-        cav.step(1)
-        cav.reduce()
+    for s in range(args.steps):
+        cav.step_monitored(1, out=mon.array[s:s + 1])
     for fs, buf in outs.items():
         cav.read(fs, out=buf.array)
     t1 = time.perf_counter()
@@ -254,7 +260,7 @@ def run_ours(args, w):
     e2e = world * nodes * args.steps / e2e_s / 1e6
     h2d = 10 * nodes * 4
     d2h = sum(b.array.nbytes for b in outs.values())
-    red = cav.reduce()
+    red = {"mass": float(mon.array[-1]["mass"]), "nonfinite": int(mon.array["nonfinite"].max())}
     cav.close()
 
     if rank != 0:
@@ -284,11 +290,12 @@ def run_ours(args, w):
                      "bytes_per_node_alg": w["b_alg"], "peak_kind": f"of {peak_kind}"},
         "e2e": {"value": round(e2e, 2), "unit": "MLUPS", "h2d_bytes_per_step": round(h2d / args.steps),
                 "d2h_bytes_per_step": round(24 + d2h / args.steps),
-                "what": "lbm_write_fields (pinned h2d) + K x (lbm_step + lbm_reduce with its 24 B read back) + "
-                        "lbm_read_fields of moments and function objects"},
+                "what": "lbm_write_fields (pinned h2d of the state) + K x lbm_step_monitored (each step's 24 B "
+                        "FP64 mass/energy/non-finite sums copied back) + lbm_read_fields of moments and "
+                        "function objects"},
         "gpu_launches": int(launches),
         "clocks": clocks,
-        "check": {"mass": red["mass"], "nonfinite": red["nonfinite"]},
+        "check": {"mass_last_step": red["mass"], "nonfinite_max": red["nonfinite"]},
         "kernel": {"tile": [info["tile_x"], info["tile_y"]], "z_chunk": info["z_chunk"], "stages": info["stages"]},
     }
     if world == 1 and not args.no_cpu_baseline:

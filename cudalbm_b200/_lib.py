@@ -30,7 +30,7 @@ F32, F64 = 0, 1
 EXPORTS = ("lbm_config_default", "lbm_create", "lbm_destroy", "lbm_init_regions", "lbm_write_fields",
            "lbm_read_fields", "lbm_step", "lbm_synchronize", "lbm_reduce", "lbm_get_info", "lbm_last_error",
            "lbm_status_string", "lbm_field_set_vars", "lbm_host_alloc", "lbm_host_free", "lbm_case_read",
-           "lbm_lbmbin_write", "lbm_reduce_moments_noalloc")
+           "lbm_lbmbin_write", "lbm_reduce_moments_noalloc", "lbm_step_monitored")
 
 
 class Config(ctypes.Structure):
@@ -55,6 +55,9 @@ class Case(ctypes.Structure):
                 ("nz", ctypes.c_uint64), ("Lx", ctypes.c_float), ("Ly", ctypes.c_float), ("Lz", ctypes.c_float),
                 ("function_objects", ctypes.c_uint32), ("region", ctypes.c_float * 70),
                 ("latest_time", ctypes.c_uint64), ("has_restart", ctypes.c_int32)]
+
+
+MONITOR_DTYPE = [("mass", "<f8"), ("rho_u2", "<f8"), ("nonfinite", "<u8")]
 
 
 class LBMError(RuntimeError):
@@ -93,11 +96,12 @@ def lib() -> ctypes.CDLL:
         L.lbm_host_free.argtypes = [vp]
         L.lbm_case_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(Case)]
         L.lbm_reduce_moments_noalloc.argtypes = [vp, u64, ctypes.POINTER(ctypes.c_double), vp]
+        L.lbm_step_monitored.argtypes = [vp, u64, vp]
         L.lbm_lbmbin_write.argtypes = [ctypes.c_char_p, u64, u64, u64, i32, ctypes.POINTER(ctypes.c_char_p), vp, u64,
                                        i32]
         for name in ("lbm_create", "lbm_destroy", "lbm_init_regions", "lbm_write_fields", "lbm_read_fields",
                      "lbm_step", "lbm_synchronize", "lbm_reduce", "lbm_get_info", "lbm_host_alloc", "lbm_host_free",
-                     "lbm_case_read", "lbm_lbmbin_write", "lbm_reduce_moments_noalloc"):
+                     "lbm_case_read", "lbm_lbmbin_write", "lbm_reduce_moments_noalloc", "lbm_step_monitored"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib

@@ -144,14 +144,15 @@ struct TileCfg {
     int tx, ty, stages;
 };
 
-template <int Q, int TX, int TY, int NS, bool FO, typename MeanT>
-struct KernelInst {
-    static constexpr size_t smem = lbm::SmemLayout<Q, TX, TY, NS>::bytes;
-    static void *fn() { return reinterpret_cast<void *>(&lbm::step_kernel<Q, TX, TY, NS, FO, MeanT>); }
-};
+template <int Q, int TX, int TY, int NS, bool FO, typename MeanT, bool MON>
+void *kernel_fn()
+{
+    return reinterpret_cast<void *>(&lbm::step_kernel<Q, TX, TY, NS, FO, MeanT, MON>);
+}
 
 struct Launcher {
-    void *fn = nullptr;
+    void *fn = nullptr;      // plain step
+    void *fn_mon = nullptr;  // step that also accumulates the per-step monitor sums
     size_t smem = 0;
     int tx = 0, ty = 0, stages = 0;
 };
@@ -163,15 +164,16 @@ Launcher pick_fo(bool fo, int mean_bits)
     l.tx = TX;
     l.ty = TY;
     l.stages = NS;
+    l.smem = lbm::SmemLayout<Q, TX, TY, NS>::bytes;
     if (!fo) {
-        l.fn = KernelInst<Q, TX, TY, NS, false, float>::fn();
-        l.smem = KernelInst<Q, TX, TY, NS, false, float>::smem;
+        l.fn = kernel_fn<Q, TX, TY, NS, false, float, false>();
+        l.fn_mon = kernel_fn<Q, TX, TY, NS, false, float, true>();
     } else if (mean_bits == 64) {
-        l.fn = KernelInst<Q, TX, TY, NS, true, double>::fn();
-        l.smem = KernelInst<Q, TX, TY, NS, true, double>::smem;
+        l.fn = kernel_fn<Q, TX, TY, NS, true, double, false>();
+        l.fn_mon = kernel_fn<Q, TX, TY, NS, true, double, true>();
     } else {
-        l.fn = KernelInst<Q, TX, TY, NS, true, float>::fn();
-        l.smem = KernelInst<Q, TX, TY, NS, true, float>::smem;
+        l.fn = kernel_fn<Q, TX, TY, NS, true, float, false>();
+        l.fn_mon = kernel_fn<Q, TX, TY, NS, true, float, true>();
     }
     return l;
 }
@@ -252,6 +254,7 @@ struct lbm_handle {
     uint64_t launches = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool timed = false;
+    lbm::MonitorSlot *mon = nullptr;  // one slot, reused by every monitored step
 };
 
 namespace {
@@ -337,11 +340,12 @@ dim3 grid_1d(size_t N)
 }
 
 template <typename MeanT>
-lbm_status launch_step(lbm_handle *h)
+lbm_status launch_step(lbm_handle *h, bool monitored = false)
 {
     StepParams<MeanT> p{};
     const int nxt = h->cur ^ 1;
     p.out = h->m[nxt];
+    p.mon = h->mon;
     p.nx = int(h->cfg.nx);
     p.ny = int(h->cfg.ny);
     p.nz = int(h->cfg.nz);
@@ -370,7 +374,8 @@ lbm_status launch_step(lbm_handle *h)
                     unsigned((h->cfg.ny + h->launcher.ty - 1) / h->launcher.ty),
                     unsigned((h->cfg.nz + h->zc - 1) / h->zc));
     void *args[] = {&h->tmap[h->cur], &p};
-    LBM_CUDA(cudaLaunchKernel(h->launcher.fn, grid, block, args, h->launcher.smem, h->stream));
+    LBM_CUDA(cudaLaunchKernel(monitored ? h->launcher.fn_mon : h->launcher.fn, grid, block, args, h->launcher.smem,
+                              h->stream));
     h->cur = nxt;
     h->t += 1;
     h->launches += 1;
@@ -500,6 +505,7 @@ lbm_status lbm_create(const lbm_config *cfg, lbm_handle **out)
         if ((s = dev_alloc(h, reinterpret_cast<char **>(&h->momentsMean), 10 * h->N * msz)) != LBM_OK) return cleanup_fail(s);
     if ((s = dev_alloc(h, &h->err, 4)) != LBM_OK) return cleanup_fail(s);
     if ((s = dev_alloc(h, &h->red, 4)) != LBM_OK) return cleanup_fail(s);
+    if ((s = dev_alloc(h, &h->mon, 1)) != LBM_OK) return cleanup_fail(s);
     for (int b = 0; b < 2; b++) {
         cudaMemsetAsync(h->m[b], 0, 10 * h->N * 4, h->stream);
     }
@@ -514,8 +520,9 @@ lbm_status lbm_create(const lbm_config *cfg, lbm_handle **out)
     for (int b = 0; b < 2; b++)
         if ((s = make_tmap(h, b)) != LBM_OK)
             return cleanup_fail(s);
-    if (cudaFuncSetAttribute(h->launcher.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(h->launcher.smem)) != cudaSuccess)
-        return cleanup_fail(fail(LBM_ERR_CUDA, "cannot reserve shared memory for the step kernel"));
+    for (void *fn : {h->launcher.fn, h->launcher.fn_mon})
+        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(h->launcher.smem)) != cudaSuccess)
+            return cleanup_fail(fail(LBM_ERR_CUDA, "cannot reserve shared memory for the step kernel"));
     *out = h;
     return LBM_OK;
 }
@@ -529,7 +536,7 @@ lbm_status lbm_destroy(lbm_handle *h)
         cudaStreamSynchronize(h->stream);
     for (void *p : {static_cast<void *>(h->m[0]), static_cast<void *>(h->m[1]), static_cast<void *>(h->S),
                     static_cast<void *>(h->k), h->SMean, h->kMean, h->momentsMean, static_cast<void *>(h->err),
-                    static_cast<void *>(h->red), h->scratch})
+                    static_cast<void *>(h->red), static_cast<void *>(h->mon), h->scratch})
         if (p)
             cudaFree(p);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -668,6 +675,28 @@ lbm_status lbm_step(lbm_handle *h, uint64_t n)
         lbm_status s = md ? launch_step<double>(h) : launch_step<float>(h);
         if (s != LBM_OK)
             return s;
+    }
+    LBM_CUDA(cudaEventRecord(h->ev1, h->stream));
+    h->timed = true;
+    return LBM_OK;
+}
+
+lbm_status lbm_step_monitored(lbm_handle *h, uint64_t n, lbm_monitor *out)
+{
+    if (!h || (!out && n))
+        return fail(LBM_ERR_ARG, "null argument");
+    LBM_CUDA(cudaSetDevice(h->cfg.device));
+    static_assert(sizeof(lbm_monitor) == sizeof(lbm::MonitorSlot), "monitor layout");
+    if (n == 0)
+        return LBM_OK;
+    LBM_CUDA(cudaEventRecord(h->ev0, h->stream));
+    const bool md = h->cfg.mean_bits == 64;
+    for (uint64_t i = 0; i < n; i++) {
+        LBM_CUDA(cudaMemsetAsync(h->mon, 0, sizeof(lbm::MonitorSlot), h->stream));
+        lbm_status s = md ? launch_step<double>(h, true) : launch_step<float>(h, true);
+        if (s != LBM_OK)
+            return s;
+        LBM_CUDA(cudaMemcpyAsync(&out[i], h->mon, sizeof(lbm::MonitorSlot), cudaMemcpyDeviceToHost, h->stream));
     }
     LBM_CUDA(cudaEventRecord(h->ev1, h->stream));
     h->timed = true;

@@ -109,9 +109,17 @@ struct FOPtrs {
     StrainDiv sd;        // divisors of S and their reciprocals
 };
 
+// Global sums of one step's result, accumulated by every CTA (FP64).
+struct MonitorSlot {
+    double mass;                   // sum of rho
+    double rho_u2;                 // sum of rho |u_stored|^2 (kinetic energy = this * 0.5 / 9)
+    unsigned long long nonfinite;  // nodes with a NaN/Inf among their 10 stored moments
+};
+
 template <typename MeanT>
 struct StepParams {
     float *out;        // [10][N] moments after the step
+    MonitorSlot *mon;  // per-step sums (monitored kernels only)
     int nx, ny, nz;
     int zc;            // z-planes per CTA
     Relax rx;
@@ -184,8 +192,8 @@ __device__ __forceinline__ void ring_pops(const float *sm, float *pb, int rx, in
 }
 
 // ---------------------------------------------------------------- kernel
-template <int Q, int TX, int TY, int NSTAGE, bool FO, typename MeanT>
-__global__ void __launch_bounds__(TX *TY) step_kernel(const __grid_constant__ CUtensorMap tmap_in, const StepParams<MeanT> p)
+template <int Q, int TX, int TY, int NSTAGE, bool FO, typename MeanT, bool MON = false>
+__global__ void __launch_bounds__(TX *TY, 2) step_kernel(const __grid_constant__ CUtensorMap tmap_in, const StepParams<MeanT> p)
 {
     using G = TileGeom<TX, TY>;
     using L = SmemLayout<Q, TX, TY, NSTAGE>;
@@ -226,6 +234,8 @@ __global__ void __launch_bounds__(TX *TY) step_kernel(const __grid_constant__ CU
 
     // populations held in registers between planes
     float U2[ZG::NU], U1[ZG::NU], S1[ZG::NS];  // U(p-2), U(p-1), S(p-1)
+    double mon_mass = 0.0, mon_ke = 0.0;
+    unsigned mon_bad = 0;
 
     for (int i = 0; i < nplanes; i++) {
         const int pz = z0 - 1 + i;  // plane being received
@@ -325,6 +335,12 @@ __global__ void __launch_bounds__(TX *TY) step_kernel(const __grid_constant__ CU
 #pragma unroll
                 for (int k = 1; k < 10; k++)
                     o[k * N] = m[k];
+                if constexpr (MON) {
+                    mon_mass += double(m[0]);
+                    mon_ke += double(m[0] * ((m[1] * m[1] + m[2] * m[2]) + m[3] * m[3]));
+                    const float chk = (((m[0] + m[1]) + (m[2] + m[3])) + ((m[4] + m[5]) + (m[6] + m[7]))) + (m[8] + m[9]);
+                    mon_bad += !isfinite(chk);
+                }
                 if constexpr (FO) {
                     if (p.fo.S || p.fo.SMean) {
                         float s6[6];
@@ -375,6 +391,36 @@ __global__ void __launch_bounds__(TX *TY) step_kernel(const __grid_constant__ CU
 #pragma unroll
         for (int k = 0; k < ZG::NS; k++)
             S1[k] = S0[k];
+    }
+
+    if constexpr (MON) {
+        // CTA sums, then one FP64 atomic per quantity
+        for (int o = 16; o > 0; o >>= 1) {
+            mon_mass += __shfl_down_sync(0xffffffffu, mon_mass, o);
+            mon_ke += __shfl_down_sync(0xffffffffu, mon_ke, o);
+            mon_bad += __shfl_down_sync(0xffffffffu, mon_bad, o);
+        }
+        __shared__ double s_mon[2][TX * TY / 32];
+        __shared__ unsigned s_bad[TX * TY / 32];
+        const int lane = lin & 31, wid = lin >> 5;
+        if (lane == 0) {
+            s_mon[0][wid] = mon_mass;
+            s_mon[1][wid] = mon_ke;
+            s_bad[wid] = mon_bad;
+        }
+        __syncthreads();
+        if (lin == 0) {
+            double a = 0.0, b = 0.0;
+            unsigned long long c = 0;
+            for (int w = 0; w < TX * TY / 32; w++) {
+                a += s_mon[0][w];
+                b += s_mon[1][w];
+                c += s_bad[w];
+            }
+            atomicAdd(&p.mon->mass, a);
+            atomicAdd(&p.mon->rho_u2, b);
+            atomicAdd(&p.mon->nonfinite, c);
+        }
     }
 
     if (s_abort) {

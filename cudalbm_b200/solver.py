@@ -105,6 +105,16 @@ class Cavity:
     def step(self, n: int = 1) -> None:
         _lib.check(_lib.lib().lbm_step(self._h, int(n)))
 
+    def step_monitored(self, n: int, out=None):
+        """n steps, each returning (mass, rho*|u_stored|^2, nonfinite) sums
+        computed by the step kernel; ``out`` is a structured array of length
+        >= n (page-locked for a fully asynchronous call).  Valid after
+        synchronize()."""
+        if out is None:
+            out = np.zeros(n, dtype=_lib.MONITOR_DTYPE)
+        _lib.check(_lib.lib().lbm_step_monitored(self._h, int(n), out.ctypes.data))
+        return out
+
     def synchronize(self) -> None:
         _lib.check(_lib.lib().lbm_synchronize(self._h))
 

@@ -130,6 +130,21 @@ lbm_status lbm_read_fields(lbm_handle *h, lbm_field_set set, void *host, size_t 
  * Asynchronous: returns after enqueueing; errors of the launches are reported. */
 lbm_status lbm_step(lbm_handle *h, uint64_t n);
 
+/* Per-step global sums, accumulated in FP64 by the step kernel itself. */
+typedef struct lbm_monitor {
+    double mass;             /* sum of rho over the nodes */
+    double rho_u2;           /* sum of rho*|u_stored|^2; kinetic energy = rho_u2 * 0.5 / 9 */
+    uint64_t nonfinite;      /* nodes with a NaN/Inf among their 10 moments (divergence watchdog) */
+} lbm_monitor;
+
+/* lbm_step with a per-step result: step i writes its sums to out[i] (n
+ * entries) by an asynchronous device-to-host copy queued after the step.
+ * With page-locked `out` (lbm_host_alloc) nothing waits for the host; the
+ * values are valid after lbm_synchronize.  Replaces: the reference's per-step
+ * info print (momentBasedD3Q19.cu:107-110) and fieldCalculate containsNaN
+ * (applications/fieldCalculate/fieldCalculate.cuh:74-110), at no extra pass. */
+lbm_status lbm_step_monitored(lbm_handle *h, uint64_t n, lbm_monitor *out);
+
 /* Wait for queued work and report device-side error flags. */
 lbm_status lbm_synchronize(lbm_handle *h);
 
