@@ -219,8 +219,9 @@ def run_ours(args, w):
     nodes = nx * ny * nz
     tile = (args.tile_x, args.tile_y, args.stages) if args.tile_x else None
     cav = Cavity(w["lattice"], nx, ny, nz, w["Re"], w["u"], function_objects=w["fo"], mean_bits=w["mean_bits"],
-                 device=local, tile=tile, z_chunk=args.z_chunk)
+                 device=local, tile=tile, z_chunk=args.z_chunk, pop_buffers=args.pop_buffers)
     cav.init_regions()
+    tuning = cav.autotune(args.tune_steps) if (not args.no_autotune and not args.tile_x) else None
     cav.step(args.warmup)
     cav.synchronize()
 
@@ -296,7 +297,8 @@ def run_ours(args, w):
         "gpu_launches": int(launches),
         "clocks": clocks,
         "check": {"mass_last_step": red["mass"], "nonfinite_max": red["nonfinite"]},
-        "kernel": {"tile": [info["tile_x"], info["tile_y"]], "z_chunk": info["z_chunk"], "stages": info["stages"]},
+        "kernel": {"tile": [info["tile_x"], info["tile_y"]], "z_chunk": info["z_chunk"], "stages": info["stages"],
+                   "autotuned": tuning},
     }
     if world == 1 and not args.no_cpu_baseline:
         try:
@@ -384,6 +386,9 @@ def main():
     ap.add_argument("--tile-y", type=int, default=8)
     ap.add_argument("--stages", type=int, default=0)
     ap.add_argument("--z-chunk", type=int, default=0)
+    ap.add_argument("--pop-buffers", type=int, default=0)
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default kernel variant")
+    ap.add_argument("--tune-steps", type=int, default=10)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

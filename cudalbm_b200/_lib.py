@@ -30,7 +30,7 @@ F32, F64 = 0, 1
 EXPORTS = ("lbm_config_default", "lbm_create", "lbm_destroy", "lbm_init_regions", "lbm_write_fields",
            "lbm_read_fields", "lbm_step", "lbm_synchronize", "lbm_reduce", "lbm_get_info", "lbm_last_error",
            "lbm_status_string", "lbm_field_set_vars", "lbm_host_alloc", "lbm_host_free", "lbm_case_read",
-           "lbm_lbmbin_write", "lbm_reduce_moments_noalloc", "lbm_step_monitored")
+           "lbm_lbmbin_write", "lbm_reduce_moments_noalloc", "lbm_step_monitored", "lbm_autotune")
 
 
 class Config(ctypes.Structure):
@@ -38,7 +38,7 @@ class Config(ctypes.Structure):
                 ("ny", ctypes.c_int64), ("nz", ctypes.c_int64), ("Re", ctypes.c_float), ("u_inf", ctypes.c_float),
                 ("function_objects", ctypes.c_uint32), ("mean_bits", ctypes.c_int32),
                 ("start_step", ctypes.c_int64), ("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32),
-                ("z_chunk", ctypes.c_int32), ("stages", ctypes.c_int32)]
+                ("z_chunk", ctypes.c_int32), ("stages", ctypes.c_int32), ("pop_buffers", ctypes.c_int32)]
 
 
 class Info(ctypes.Structure):
@@ -46,6 +46,12 @@ class Info(ctypes.Structure):
                 ("omega", ctypes.c_float), ("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32),
                 ("z_chunk", ctypes.c_int32), ("stages", ctypes.c_int32), ("device_bytes", ctypes.c_uint64),
                 ("last_step_ms", ctypes.c_double), ("kernel_launches", ctypes.c_uint64)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32), ("z_chunk", ctypes.c_int32),
+                ("stages", ctypes.c_int32), ("pop_buffers", ctypes.c_int32), ("ms_per_step", ctypes.c_double),
+                ("candidates", ctypes.c_int32), ("from_cache", ctypes.c_int32)]
 
 
 class Case(ctypes.Structure):
@@ -97,11 +103,12 @@ def lib() -> ctypes.CDLL:
         L.lbm_case_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(Case)]
         L.lbm_reduce_moments_noalloc.argtypes = [vp, u64, ctypes.POINTER(ctypes.c_double), vp]
         L.lbm_step_monitored.argtypes = [vp, u64, vp]
+        L.lbm_autotune.argtypes = [vp, i32, ctypes.POINTER(Tuning)]
         L.lbm_lbmbin_write.argtypes = [ctypes.c_char_p, u64, u64, u64, i32, ctypes.POINTER(ctypes.c_char_p), vp, u64,
                                        i32]
         for name in ("lbm_create", "lbm_destroy", "lbm_init_regions", "lbm_write_fields", "lbm_read_fields",
                      "lbm_step", "lbm_synchronize", "lbm_reduce", "lbm_get_info", "lbm_host_alloc", "lbm_host_free",
-                     "lbm_case_read", "lbm_lbmbin_write", "lbm_reduce_moments_noalloc", "lbm_step_monitored"):
+                     "lbm_case_read", "lbm_lbmbin_write", "lbm_reduce_moments_noalloc", "lbm_step_monitored", "lbm_autotune"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib

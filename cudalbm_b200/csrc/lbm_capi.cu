@@ -12,6 +12,7 @@
 #include <array>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -144,55 +145,76 @@ struct TileCfg {
     int tx, ty, stages;
 };
 
-template <int Q, int TX, int TY, int NS, bool FO, typename MeanT, bool MON>
+template <int Q, int TX, int TY, int NS, bool FO, typename MeanT, bool MON, int NPB, int MINB>
 void *kernel_fn()
 {
-    return reinterpret_cast<void *>(&lbm::step_kernel<Q, TX, TY, NS, FO, MeanT, MON>);
+    return reinterpret_cast<void *>(&lbm::step_kernel<Q, TX, TY, NS, FO, MeanT, MON, NPB, MINB>);
 }
 
 struct Launcher {
     void *fn = nullptr;      // plain step
     void *fn_mon = nullptr;  // step that also accumulates the per-step monitor sums
     size_t smem = 0;
-    int tx = 0, ty = 0, stages = 0;
+    int tx = 0, ty = 0, stages = 0, pop_buffers = 2;
 };
 
-template <int Q, int TX, int TY, int NS>
+template <int Q, int TX, int TY, int NS, int NPB = 2, int MINB = 2>
 Launcher pick_fo(bool fo, int mean_bits)
 {
     Launcher l;
     l.tx = TX;
     l.ty = TY;
     l.stages = NS;
-    l.smem = lbm::SmemLayout<Q, TX, TY, NS>::bytes;
+    l.pop_buffers = NPB;
+    l.smem = lbm::SmemLayout<Q, TX, TY, NS, NPB>::bytes;
     if (!fo) {
-        l.fn = kernel_fn<Q, TX, TY, NS, false, float, false>();
-        l.fn_mon = kernel_fn<Q, TX, TY, NS, false, float, true>();
+        l.fn = kernel_fn<Q, TX, TY, NS, false, float, false, NPB, MINB>();
+        l.fn_mon = kernel_fn<Q, TX, TY, NS, false, float, true, NPB, MINB>();
     } else if (mean_bits == 64) {
-        l.fn = kernel_fn<Q, TX, TY, NS, true, double, false>();
-        l.fn_mon = kernel_fn<Q, TX, TY, NS, true, double, true>();
+        l.fn = kernel_fn<Q, TX, TY, NS, true, double, false, NPB, MINB>();
+        l.fn_mon = kernel_fn<Q, TX, TY, NS, true, double, true, NPB, MINB>();
     } else {
-        l.fn = kernel_fn<Q, TX, TY, NS, true, float, false>();
-        l.fn_mon = kernel_fn<Q, TX, TY, NS, true, float, true>();
+        l.fn = kernel_fn<Q, TX, TY, NS, true, float, false, NPB, MINB>();
+        l.fn_mon = kernel_fn<Q, TX, TY, NS, true, float, true, NPB, MINB>();
     }
     return l;
 }
 
 // Available tile shapes.  The first entry per lattice is the default for
 // large meshes; narrower tiles serve meshes whose nx is not a multiple of 32.
-bool pick_launcher(int Q, int tx, int ty, int stages, bool fo, int mean_bits, Launcher &out)
+// Every compiled kernel variant: (lattice, tile x, tile y, TMA stages,
+// population-plane code).  Population-plane code 1 = one plane, 3 CTAs/SM;
+// 2 = two planes, 2 CTAs/SM; 4 = one plane, 4 CTAs/SM.
+struct Variant {
+    int Q, tx, ty, stages, npb;
+};
+const Variant kVariants[] = {{19, 32, 8, 2, 1}, {19, 32, 8, 3, 1}, {19, 32, 8, 3, 2}, {19, 32, 8, 2, 2},
+                             {19, 32, 8, 2, 4}, {19, 16, 8, 2, 1}, {19, 8, 8, 2, 1},  {27, 32, 8, 2, 1},
+                             {27, 32, 8, 2, 2}, {27, 16, 8, 2, 1}, {27, 8, 8, 2, 1}};
+
+bool pick_launcher(int Q, int tx, int ty, int stages, int npb, bool fo, int mean_bits, Launcher &out)
 {
-#define LBM_TRY(QQ, TXX, TYY, NSS)                          \
-    if (Q == QQ && tx == TXX && ty == TYY && stages == NSS) { \
-        out = pick_fo<QQ, TXX, TYY, NSS>(fo, mean_bits);      \
-        return true;                                          \
+#define LBM_TRY(QQ, TXX, TYY, NSS, NPB, MINB)                                    \
+    if (Q == QQ && tx == TXX && ty == TYY && stages == NSS && npb == NPB) {      \
+        out = pick_fo<QQ, TXX, TYY, NSS, NPB, MINB>(fo, mean_bits);              \
+        return true;                                                             \
     }
-    LBM_TRY(19, 32, 8, 3)
-    LBM_TRY(19, 16, 8, 3)
-    LBM_TRY(19, 8, 8, 3)
-    LBM_TRY(27, 32, 8, 2)
-    LBM_TRY(27, 16, 8, 2)
-    LBM_TRY(27, 8, 8, 2)
+    // (lattice, tile x, tile y, TMA stages, population planes, min CTAs/SM)
+    LBM_TRY(19, 32, 8, 2, 1, 3)
+    LBM_TRY(19, 32, 8, 3, 1, 3)
+    LBM_TRY(19, 32, 8, 3, 2, 2)
+    LBM_TRY(19, 32, 8, 2, 2, 2)
+    if (Q == 19 && tx == 32 && ty == 8 && stages == 2 && npb == 4) {  // 1 plane, 4 CTAs/SM (experimental)
+        out = pick_fo<19, 32, 8, 2, 1, 4>(fo, mean_bits);
+        out.pop_buffers = 4;
+        return true;
+    }
+    LBM_TRY(19, 16, 8, 2, 1, 3)
+    LBM_TRY(19, 8, 8, 2, 1, 3)
+    LBM_TRY(27, 32, 8, 2, 1, 3)
+    LBM_TRY(27, 32, 8, 2, 2, 2)
+    LBM_TRY(27, 16, 8, 2, 1, 3)
+    LBM_TRY(27, 8, 8, 2, 1, 3)
 #undef LBM_TRY
     return false;
 }
@@ -201,9 +223,10 @@ bool pick_launcher(int Q, int tx, int ty, int stages, bool fo, int mean_bits, La
 // sized so that the grid holds several waves of CTAs on 148 SMs.
 void default_tiling(int Q, int64_t nx, int64_t ny, int64_t nz, int &tx, int &ty, int &zc, int &stages)
 {
+    (void)Q;
     tx = (nx % 32 == 0) ? 32 : (nx % 16 == 0 ? 16 : 8);
     ty = 8;
-    stages = Q == 19 ? 3 : 2;
+    stages = 2;
     const int64_t tiles = ((nx + tx - 1) / tx) * ((ny + ty - 1) / ty);
     int64_t c = nz;
     while (c > 16 && tiles * ((nz + c - 1) / c) < 8 * 148)
@@ -473,7 +496,8 @@ lbm_status lbm_create(const lbm_config *cfg, lbm_handle **out)
     if (c.z_chunk) zc = c.z_chunk;
     if (c.stages) st = c.stages;
     const bool fo = c.function_objects != 0;
-    if (!pick_launcher(h->Q, tx, ty, st, fo, c.mean_bits, h->launcher)) {
+    const int npb = c.pop_buffers ? c.pop_buffers : 1;
+    if (!pick_launcher(h->Q, tx, ty, st, npb, fo, c.mean_bits, h->launcher)) {
         delete h;
         return fail(LBM_ERR_ARG, "unsupported tile configuration");
     }
@@ -802,6 +826,211 @@ lbm_status lbm_host_free(void *p)
 {
     if (p)
         LBM_CUDA(cudaFreeHost(p));
+    return LBM_OK;
+}
+
+// ------------------------------------------------------------- autotuner
+namespace {
+
+struct TuneKey {
+    int Q;
+    int64_t nx, ny, nz;
+    uint32_t fo;
+    int mean_bits;
+    bool operator==(const TuneKey &o) const
+    {
+        return Q == o.Q && nx == o.nx && ny == o.ny && nz == o.nz && fo == o.fo && mean_bits == o.mean_bits;
+    }
+};
+struct TuneEntry {
+    TuneKey key;
+    lbm_tuning best;
+};
+std::mutex g_tune_mu;
+std::vector<TuneEntry> g_tune_cache;
+
+const char *tune_cache_path()
+{
+    const char *p = std::getenv("LBM_B200_TUNE_CACHE");
+    return (p && *p) ? p : nullptr;
+}
+
+void load_tune_file()
+{
+    static bool loaded = false;
+    if (loaded)
+        return;
+    loaded = true;
+    const char *path = tune_cache_path();
+    if (!path)
+        return;
+    FILE *f = std::fopen(path, "r");
+    if (!f)
+        return;
+    TuneEntry e{};
+    long long nx, ny, nz;
+    unsigned fo;
+    while (std::fscanf(f, "%d %lld %lld %lld %u %d %d %d %d %d %d %lf", &e.key.Q, &nx, &ny, &nz, &fo, &e.key.mean_bits,
+                       &e.best.tile_x, &e.best.tile_y, &e.best.stages, &e.best.pop_buffers, &e.best.z_chunk,
+                       &e.best.ms_per_step) == 12) {
+        e.key.nx = nx;
+        e.key.ny = ny;
+        e.key.nz = nz;
+        e.key.fo = fo;
+        g_tune_cache.push_back(e);
+    }
+    std::fclose(f);
+}
+
+void save_tune_entry(const TuneEntry &e)
+{
+    const char *path = tune_cache_path();
+    if (!path)
+        return;
+    FILE *f = std::fopen(path, "a");
+    if (!f)
+        return;
+    std::fprintf(f, "%d %lld %lld %lld %u %d %d %d %d %d %d %.6f\n", e.key.Q, (long long)e.key.nx, (long long)e.key.ny,
+                 (long long)e.key.nz, e.key.fo, e.key.mean_bits, e.best.tile_x, e.best.tile_y, e.best.stages,
+                 e.best.pop_buffers, e.best.z_chunk, e.best.ms_per_step);
+    std::fclose(f);
+}
+
+// Switch the handle to another kernel variant (same results, other speed).
+lbm_status apply_variant(lbm_handle *h, int tx, int ty, int stages, int npb, int zc)
+{
+    Launcher l;
+    if (!pick_launcher(h->Q, tx, ty, stages, npb, h->cfg.function_objects != 0, h->cfg.mean_bits, l))
+        return fail(LBM_ERR_ARG, "unsupported tile configuration");
+    for (void *fn : {l.fn, l.fn_mon})
+        LBM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(l.smem)));
+    h->launcher = l;
+    h->zc = std::max(1, std::min<int>(zc, int(h->cfg.nz)));
+    for (int b = 0; b < 2; b++) {
+        lbm_status s = make_tmap(h, b);
+        if (s != LBM_OK)
+            return s;
+    }
+    return LBM_OK;
+}
+
+}  // namespace
+
+lbm_status lbm_autotune(lbm_handle *h, int32_t trial_steps, lbm_tuning *out)
+{
+    if (!h)
+        return fail(LBM_ERR_ARG, "null handle");
+    LBM_CUDA(cudaSetDevice(h->cfg.device));
+    if (trial_steps <= 0)
+        trial_steps = 10;
+    const TuneKey key{h->Q, h->cfg.nx, h->cfg.ny, h->cfg.nz, h->cfg.function_objects, h->cfg.mean_bits};
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        load_tune_file();
+        for (const auto &e : g_tune_cache)
+            if (e.key == key) {
+                lbm_status s = apply_variant(h, e.best.tile_x, e.best.tile_y, e.best.stages, e.best.pop_buffers,
+                                             e.best.z_chunk);
+                if (s != LBM_OK)
+                    return s;
+                if (out) {
+                    *out = e.best;
+                    out->from_cache = 1;
+                }
+                return LBM_OK;
+            }
+    }
+    // back up the state the trials will advance
+    const size_t msz = h->cfg.mean_bits == 64 ? 8 : 4;
+    std::vector<std::pair<void *, size_t>> live = {{h->m[h->cur], 10 * h->N * 4}};
+    if (h->S) live.push_back({h->S, 6 * h->N * 4});
+    if (h->k) live.push_back({h->k, h->N * 4});
+    if (h->SMean) live.push_back({h->SMean, 6 * h->N * msz});
+    if (h->kMean) live.push_back({h->kMean, h->N * msz});
+    if (h->momentsMean) live.push_back({h->momentsMean, 10 * h->N * msz});
+    std::vector<void *> backup(live.size(), nullptr);
+    auto release = [&]() {
+        for (void *p : backup)
+            if (p)
+                cudaFree(p);
+    };
+    for (size_t i = 0; i < live.size(); i++) {
+        if (cudaMalloc(&backup[i], live[i].second) != cudaSuccess) {
+            release();
+            return fail(LBM_ERR_NOMEM, "autotune: no room to back up the state");
+        }
+        cudaMemcpyAsync(backup[i], live[i].first, live[i].second, cudaMemcpyDeviceToDevice, h->stream);
+    }
+    const int cur0 = h->cur;
+    const int64_t t0 = h->t;
+    const uint64_t launches0 = h->launches;
+    auto restore = [&]() {
+        h->cur = cur0;
+        h->t = t0;
+        live[0].first = h->m[cur0];
+        for (size_t i = 0; i < live.size(); i++)
+            cudaMemcpyAsync(live[i].first, backup[i], live[i].second, cudaMemcpyDeviceToDevice, h->stream);
+    };
+    const bool md = h->cfg.mean_bits == 64;
+    lbm_tuning best{};
+    best.ms_per_step = 1e30;
+    int tried = 0;
+    const int zcs[] = {8, 16, 32, 64};
+    for (const Variant &v : kVariants) {
+        if (v.Q != h->Q || v.tx > h->cfg.nx || v.ty > h->cfg.ny)
+            continue;
+        for (int zc : zcs) {
+            if (zc > h->cfg.nz)
+                continue;
+            lbm_status s = apply_variant(h, v.tx, v.ty, v.stages, v.npb, zc);
+            if (s != LBM_OK) {
+                release();
+                return s;
+            }
+            for (int w = 0; w < 2 && s == LBM_OK; w++)
+                s = md ? launch_step<double>(h) : launch_step<float>(h);
+            cudaEventRecord(h->ev0, h->stream);
+            for (int k = 0; k < trial_steps && s == LBM_OK; k++)
+                s = md ? launch_step<double>(h) : launch_step<float>(h);
+            cudaEventRecord(h->ev1, h->stream);
+            float ms = 0.0f;
+            if (s == LBM_OK && cudaEventSynchronize(h->ev1) == cudaSuccess &&
+                cudaEventElapsedTime(&ms, h->ev0, h->ev1) == cudaSuccess) {
+                const double per = double(ms) / trial_steps;
+                if (per < best.ms_per_step) {
+                    best.ms_per_step = per;
+                    best.tile_x = v.tx;
+                    best.tile_y = v.ty;
+                    best.stages = v.stages;
+                    best.pop_buffers = v.npb;
+                    best.z_chunk = zc;
+                }
+                tried++;
+            }
+            restore();
+            if (s != LBM_OK) {
+                release();
+                return s;
+            }
+        }
+    }
+    lbm_status s = tried ? apply_variant(h, best.tile_x, best.tile_y, best.stages, best.pop_buffers, best.z_chunk)
+                         : fail(LBM_ERR_STATE, "autotune: no kernel variant fits this mesh");
+    LBM_CUDA(cudaStreamSynchronize(h->stream));
+    release();
+    (void)launches0;
+    h->timed = false;
+    if (s != LBM_OK)
+        return s;
+    best.candidates = tried;
+    best.from_cache = 0;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tune_cache.push_back({key, best});
+        save_tune_entry({key, best});
+    }
+    if (out)
+        *out = best;
     return LBM_OK;
 }
 

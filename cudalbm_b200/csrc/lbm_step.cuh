@@ -140,7 +140,9 @@ struct TileGeom {
     static_assert(PLANE_BYTES % 128 == 0, "stage size must keep 128 B alignment");
 };
 
-template <int Q, int TX, int TY, int NSTAGE>
+// NPB population planes: 2 lets consecutive planes overlap with one barrier
+// per plane; 1 saves shared memory (more CTAs per SM) at a second barrier.
+template <int Q, int TX, int TY, int NSTAGE, int NPB = 2>
 struct SmemLayout {
     using G = TileGeom<TX, TY>;
     static constexpr int NXY = XY<Q>::N;
@@ -148,7 +150,7 @@ struct SmemLayout {
     static constexpr size_t stage_off = 128;
     static constexpr size_t pop_off = stage_off + size_t(NSTAGE) * G::PLANE_BYTES;
     static constexpr size_t pop_floats = size_t(NXY) * G::PY * G::PX;
-    static constexpr size_t bytes = pop_off + 2 * pop_floats * 4;
+    static constexpr size_t bytes = pop_off + NPB * pop_floats * 4;
 };
 
 // directions grouped by cz: U (cz = +1), S (cz = 0, rest included), D (cz = -1)
@@ -192,11 +194,11 @@ __device__ __forceinline__ void ring_pops(const float *sm, float *pb, int rx, in
 }
 
 // ---------------------------------------------------------------- kernel
-template <int Q, int TX, int TY, int NSTAGE, bool FO, typename MeanT, bool MON = false>
-__global__ void __launch_bounds__(TX *TY, 2) step_kernel(const __grid_constant__ CUtensorMap tmap_in, const StepParams<MeanT> p)
+template <int Q, int TX, int TY, int NSTAGE, bool FO, typename MeanT, bool MON = false, int NPB = 2, int MINB = 2>
+__global__ void __launch_bounds__(TX *TY, MINB) step_kernel(const __grid_constant__ CUtensorMap tmap_in, const StepParams<MeanT> p)
 {
     using G = TileGeom<TX, TY>;
-    using L = SmemLayout<Q, TX, TY, NSTAGE>;
+    using L = SmemLayout<Q, TX, TY, NSTAGE, NPB>;
     using ZG = ZGroups<Q>;
     constexpr int NXY = XY<Q>::N;
 
@@ -242,7 +244,7 @@ __global__ void __launch_bounds__(TX *TY, 2) step_kernel(const __grid_constant__
         const int stage = i % NSTAGE;
         const unsigned parity = (i / NSTAGE) & 1;
         float *sm = stages + stage * G::PLANE_FLOATS;
-        float *pb = pops + (i & 1) * L::pop_floats;
+        float *pb = pops + (NPB == 2 ? (i & 1) : 0) * L::pop_floats;
 
         // running means of the node updated in this iteration (plane pz-1),
         // loaded early so the latency hides behind the reconstruction
@@ -391,6 +393,8 @@ __global__ void __launch_bounds__(TX *TY, 2) step_kernel(const __grid_constant__
 #pragma unroll
         for (int k = 0; k < ZG::NS; k++)
             S1[k] = S0[k];
+        if constexpr (NPB == 1)
+            __syncthreads();  // the single population plane is rewritten next iteration
     }
 
     if constexpr (MON) {

@@ -31,7 +31,7 @@ class Cavity:
 
     def __init__(self, lattice: int, nx: int, ny: int, nz: int, Re: float, u_inf: float,
                  function_objects: Iterable[str] = (), mean_bits: int = 32, device: int = 0,
-                 start_step: int = 0, tile: Optional[tuple] = None, z_chunk: int = 0):
+                 start_step: int = 0, tile: Optional[tuple] = None, z_chunk: int = 0, pop_buffers: int = 0):
         L = _lib.lib()
         cfg = _lib.Config()
         L.lbm_config_default(ctypes.byref(cfg))
@@ -50,6 +50,7 @@ class Cavity:
             if len(tile) > 2:
                 cfg.stages = int(tile[2])
         cfg.z_chunk = int(z_chunk)
+        cfg.pop_buffers = int(pop_buffers)
         self.cfg = cfg
         self.shape = (nz, ny, nx)
         self.mean_bits = mean_bits
@@ -114,6 +115,12 @@ class Cavity:
             out = np.zeros(n, dtype=_lib.MONITOR_DTYPE)
         _lib.check(_lib.lib().lbm_step_monitored(self._h, int(n), out.ctypes.data))
         return out
+
+    def autotune(self, trial_steps: int = 10) -> Dict[str, object]:
+        """Pick the fastest kernel variant for this size class (state unchanged)."""
+        t = _lib.Tuning()
+        _lib.check(_lib.lib().lbm_autotune(self._h, int(trial_steps), ctypes.byref(t)))
+        return {f: getattr(t, f) for f, _ in t._fields_}
 
     def synchronize(self) -> None:
         _lib.check(_lib.lib().lbm_synchronize(self._h))

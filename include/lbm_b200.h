@@ -79,6 +79,7 @@ typedef struct lbm_config {
     int64_t start_step;       /* absolute step index of the initial state (restart: latestTime) */
     /* kernel tiling; 0 = autotuned choice for this size class */
     int32_t tile_x, tile_y, z_chunk, stages;
+    int32_t pop_buffers;      /* shared-memory population planes: 2 (one barrier per plane) or 1 */
 } lbm_config;
 
 typedef struct lbm_handle lbm_handle;
@@ -154,6 +155,28 @@ lbm_status lbm_synchronize(lbm_handle *h);
 lbm_status lbm_reduce(lbm_handle *h, double out[3]);
 
 lbm_status lbm_get_info(lbm_handle *h, lbm_info *info);
+
+/* Kernel variant chosen by lbm_autotune. */
+typedef struct lbm_tuning {
+    int32_t tile_x, tile_y;   /* x-y tile of one CTA */
+    int32_t z_chunk;          /* z-planes per CTA */
+    int32_t stages;           /* TMA pipeline depth (moment planes in flight) */
+    int32_t pop_buffers;      /* 1: one population plane, 3 CTAs/SM; 2: two planes; 4: one plane, 4 CTAs/SM */
+    double ms_per_step;       /* measured device time per step of the chosen variant */
+    int32_t candidates;       /* variants timed */
+    int32_t from_cache;       /* 1 if taken from the cache without timing */
+} lbm_tuning;
+
+/* Time every compiled kernel variant (tile shape, pipeline depth, population
+ * planes) and z-chunk length on this handle's own state for `trial_steps`
+ * steps each, keep the fastest, and restore the state (moments, function
+ * objects and step counter) so the run continues as if nothing happened --
+ * every variant computes the same bits.  Results are cached per size class
+ * (lattice, mesh, function objects, mean precision) in the process, and in
+ * the file named by LBM_B200_TUNE_CACHE if set.  Allocates a temporary copy
+ * of the state.  Replaces: nothing in the reference, whose tiling is fixed at
+ * 8^3 (src/hardwareConfig.cuh:64-95). */
+lbm_status lbm_autotune(lbm_handle *h, int32_t trial_steps, lbm_tuning *out);
 
 /* The sums of lbm_reduce over a caller-owned device array of moments
  * ([10][nodes] floats in the stored units, on the calling thread's current

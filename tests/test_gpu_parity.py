@@ -61,9 +61,8 @@ def test_bitwise_equal_to_reference_golden(name):
 @pytest.mark.parametrize("z_chunk", [0, 8, 5])
 def test_tiling_and_chunking_do_not_change_results(q, tile, z_chunk):
     """Every tile shape and z-chunk length computes the same bits."""
-    stages = 3 if q == 19 else 2
-    base = run_cavity(q, 32, 24, 40, 400.0, 0.05, 30, fo=("S", "kMean"), tile=(32, 8, stages))
-    out = run_cavity(q, 32, 24, 40, 400.0, 0.05, 30, fo=("S", "kMean"), tile=(tile[0], tile[1], stages),
+    base = run_cavity(q, 32, 24, 40, 400.0, 0.05, 30, fo=("S", "kMean"), tile=(32, 8, 2), pop_buffers=2)
+    out = run_cavity(q, 32, 24, 40, 400.0, 0.05, 30, fo=("S", "kMean"), tile=(tile[0], tile[1], 2),
                      z_chunk=z_chunk)
     for k in base:
         assert bits_equal(out[k], base[k]), k
@@ -224,3 +223,26 @@ def test_monitored_steps_match_plain_steps_and_reduction(q, fo):
     assert mon2["nonfinite"][0] >= 1
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("q,fo", [(19, ()), (27, ("S", "SMean", "kMean"))])
+def test_autotune_leaves_the_state_untouched(q, fo):
+    """Tuning runs trial steps on the live state and restores it: tuning and
+    then stepping gives the same bits as stepping alone."""
+    a = Cavity(q, 64, 32, 48, 300.0, 0.05, function_objects=fo)
+    b = Cavity(q, 64, 32, 48, 300.0, 0.05, function_objects=fo)
+    for c in (a, b):
+        c.init_regions()
+        c.step(5)
+    t = b.autotune(3)
+    assert t["candidates"] >= 2 and t["ms_per_step"] > 0
+    for c in (a, b):
+        c.step(9)
+        c.synchronize()
+    assert b.info()["step"] == 14
+    for key in ("moments",) + tuple(fo):
+        assert bits_equal(a.read(key), b.read(key)), key
+    again = Cavity(q, 64, 32, 48, 300.0, 0.05, function_objects=fo)
+    assert again.autotune(3)["from_cache"] == 1
+    for c in (a, b, again):
+        c.close()
