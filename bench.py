@@ -68,6 +68,12 @@ WORKLOADS = {
                        desc="D3Q27 lid-driven cavity 128^3, Re=1000, function objects S/SMean/k/kMean (profiling size)"),
     "q19_128": dict(lattice=19, n=(128, 128, 128), Re=1000.0, u=0.05, fo=(), mean_bits=32, b_alg=110,
                     desc="D3Q19 lid-driven cavity 128^3, Re=1000 (profiling size)"),
+    "q19_768": dict(lattice=19, n=(768, 768, 768), Re=1000.0, u=0.05, fo=(), mean_bits=32, b_alg=110,
+                    desc="D3Q19 lid-driven cavity 768^3, Re=1000, u_lid=0.05, FP32 moments"),
+    "q19_768_f16": dict(lattice=19, n=(768, 768, 768), Re=1000.0, u=0.05, fo=(), mean_bits=32, b_alg=55,
+                        storage="f16", desc="D3Q19 lid-driven cavity 768^3, Re=1000, u_lid=0.05, FP16 moment storage"),
+    "q19_768_bf16": dict(lattice=19, n=(768, 768, 768), Re=1000.0, u=0.05, fo=(), mean_bits=32, b_alg=55,
+                         storage="bf16", desc="D3Q19 lid-driven cavity 768^3, Re=1000, u_lid=0.05, BF16 moment storage"),
     "q27_256_fo64": dict(lattice=27, n=(256, 256, 256), Re=1000.0, u=0.05, fo=("S", "SMean", "k", "kMean"),
                          mean_bits=64, b_alg=274,
                          desc="D3Q27 lid-driven cavity 256^3, Re=1000, function objects with FP64 means"),
@@ -219,7 +225,8 @@ def run_ours(args, w):
     nodes = nx * ny * nz
     tile = (args.tile_x, args.tile_y, args.stages) if args.tile_x else None
     cav = Cavity(w["lattice"], nx, ny, nz, w["Re"], w["u"], function_objects=w["fo"], mean_bits=w["mean_bits"],
-                 device=local, tile=tile, z_chunk=args.z_chunk, pop_buffers=args.pop_buffers)
+                 device=local, tile=tile, z_chunk=args.z_chunk, pop_buffers=args.pop_buffers,
+                 storage=w.get("storage", "f32"))
     cav.init_regions()
     tuning = cav.autotune(args.tune_steps) if (not args.no_autotune and not args.tile_x) else None
     cav.step(args.warmup)
@@ -242,7 +249,7 @@ def run_ours(args, w):
     value = world * nodes * args.steps / (ms / 1e3) / 1e6
 
     # ---- end to end through the C ABI with pinned host buffers (e2e)
-    state = _lib.PinnedArray((10, nz, ny, nx), np.float32)
+    state = _lib.PinnedArray((10, nz, ny, nx), np.float32)  # host values are FP32 for every storage format
     cav.read("moments", out=state.array)
     outs = {fs: _lib.PinnedArray((NVARS[fs], nz, ny, nx), np.float64 if (w["mean_bits"] == 64 and "Mean" in fs)
                                  else np.float32) for fs in ("moments",) + tuple(w["fo"])}
@@ -280,12 +287,15 @@ def run_ours(args, w):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32",
+        "dtype": {"f32": "f32", "f16": "f16 storage, f32 arithmetic", "bf16": "bf16 storage, f32 arithmetic"}[
+            w.get("storage", "f32")],
         "data": "synthetic: the lid-driven cavity initial state generated from the case's region values",
         "config": {"workload": w["desc"], "lattice": f"D3Q{w['lattice']}", "nx": nx, "ny": ny, "nz": nz,
                    "Re": w["Re"], "u_lid": w["u"], "function_objects": list(w["fo"]),
                    "mean_bits": w["mean_bits"], "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (moment buffers %.2f GB vs 126 MB L2); no flush" % (2 * 40 * nodes / 1e9)},
+                   "storage": w.get("storage", "f32"),
+                   "l2": "inputs larger than L2 (moment buffers %.2f GB vs 126 MB L2); no flush" % (
+                       2 * 10 * (2 if w.get("storage", "f32") != "f32" else 4) * nodes / 1e9)},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": (round(tpn * nodes) if tpn else None),
                      "bytes_per_node_alg": w["b_alg"], "peak_kind": f"of {peak_kind}"},

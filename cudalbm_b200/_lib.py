@@ -38,7 +38,11 @@ class Config(ctypes.Structure):
                 ("ny", ctypes.c_int64), ("nz", ctypes.c_int64), ("Re", ctypes.c_float), ("u_inf", ctypes.c_float),
                 ("function_objects", ctypes.c_uint32), ("mean_bits", ctypes.c_int32),
                 ("start_step", ctypes.c_int64), ("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32),
-                ("z_chunk", ctypes.c_int32), ("stages", ctypes.c_int32), ("pop_buffers", ctypes.c_int32)]
+                ("z_chunk", ctypes.c_int32), ("stages", ctypes.c_int32), ("pop_buffers", ctypes.c_int32),
+                ("storage", ctypes.c_int32)]
+
+
+STORAGE = {"f32": 0, "f16": 1, "bf16": 2}
 
 
 class Info(ctypes.Structure):

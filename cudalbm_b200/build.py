@@ -27,7 +27,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-cudart", "static",
               "-I" + INCLUDE, "-I" + CSRC] + ARCH
 
-LIB_SOURCES = ["lbm_capi.cu", "lbm_noalloc.cu", "casefile.cpp", "lbmbin.cpp"]
+LIB_SOURCES = ["lbm_capi.cu", "variants_q19_f32.cu", "variants_q27_f32.cu", "variants_f16.cu", "variants_bf16.cu",
+               "lbm_noalloc.cu", "casefile.cpp", "lbmbin.cpp"]
 
 
 def _nvcc() -> str:
@@ -54,14 +55,24 @@ def _run(cmd):
 
 
 def build_library(force: bool = False, verbose_ptxas: bool = False) -> str:
-    srcs = [os.path.join(CSRC, s) for s in LIB_SOURCES]
-    if force or _stale(LIB, _deps()):
-        os.makedirs(os.path.dirname(LIB), exist_ok=True)
-        cmd = [_nvcc()] + NVCC_FLAGS + ["-shared"] + srcs + ["-o", LIB + ".tmp"]
+    """Compile every source to an object in parallel, then link the library."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    if not (force or _stale(LIB, _deps())):
+        return LIB
+    objdir = os.path.join(HERE, "lib", "obj")
+    os.makedirs(objdir, exist_ok=True)
+    jobs = []
+    for src in LIB_SOURCES:
+        obj = os.path.join(objdir, src + ".o")
+        cmd = [_nvcc()] + NVCC_FLAGS + ["-c", os.path.join(CSRC, src), "-o", obj]
         if verbose_ptxas:
             cmd += ["-Xptxas", "-v"]
-        _run(cmd)
-        os.replace(LIB + ".tmp", LIB)
+        jobs.append((cmd, obj))
+    with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as pool:
+        list(pool.map(lambda j: _run(j[0]), jobs))
+    _run([_nvcc()] + NVCC_FLAGS + ["-shared"] + [o for _, o in jobs] + ["-o", LIB + ".tmp"])
+    os.replace(LIB + ".tmp", LIB)
     return LIB
 
 

@@ -24,6 +24,7 @@
 #include "lbm_b200.h"
 #include "lbm_step.cuh"
 #include "lbmbin.hpp"
+#include "lbm_variants.cuh"
 
 namespace {
 
@@ -44,7 +45,8 @@ lbm_status fail(lbm_status s, const std::string &msg)
     } while (0)
 
 // ---------------------------------------------------------------- kernels
-__global__ void init_regions_kernel(float *m, int nx, int ny, int nz, const float *region)
+template <typename ST>
+__global__ void init_regions_kernel(ST *m, int nx, int ny, int nz, const float *region)
 {
     // src/array/hostArray.cuh:304-359, evaluated in float as the reference does
     // (its "front" is z == 0 and "back" z == nz-1 there).
@@ -58,7 +60,7 @@ __global__ void init_regions_kernel(float *m, int nx, int ny, int nz, const floa
             const float *r = region + 7 * f;
             const float sum = (float(w) * r[4]) + (float(e) * r[3]) + (float(s) * r[2]) + (float(n) * r[1]) +
                               (float(fr) * r[5]) + (float(b) * r[6]);
-            m[f * N + i] = count > 0 ? sum / float(count) : r[0];
+            m[f * N + i] = lbm::Storage<ST>::store(count > 0 ? sum / float(count) : r[0], f);
         }
     }
 }
@@ -67,6 +69,31 @@ __device__ __forceinline__ size_t tiled_index(int x, int y, int z, int nbx, int 
 {
     const int tx = x & 7, ty = y & 7, tz = z & 7, bx = x >> 3, by = y >> 3, bz = z >> 3;
     return size_t(tx) + 8 * (size_t(ty) + 8 * (size_t(tz) + 8 * (size_t(bx) + size_t(nbx) * (size_t(by) + size_t(nby) * bz))));
+}
+
+// One moment field between host values (reference convention, order/type of
+// the host buffer) and the device storage format of field k.
+template <typename ST, typename H>
+__global__ void moment_in_kernel(ST *dst, const H *src, int k, int nx, int ny, int nz, int tiled)
+{
+    const size_t N = size_t(nx) * ny * nz;
+    const int nbx = nx / 8, nby = ny / 8;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x) {
+        const int x = int(i % nx), y = int((i / nx) % ny), z = int(i / (size_t(nx) * ny));
+        const size_t j = tiled ? tiled_index(x, y, z, nbx, nby) : i;
+        dst[i] = lbm::Storage<ST>::store(float(src[j]), k);
+    }
+}
+template <typename ST, typename H>
+__global__ void moment_out_kernel(H *dst, const ST *src, int k, int nx, int ny, int nz, int tiled)
+{
+    const size_t N = size_t(nx) * ny * nz;
+    const int nbx = nx / 8, nby = ny / 8;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x) {
+        const int x = int(i % nx), y = int((i / nx) % ny), z = int(i / (size_t(nx) * ny));
+        const size_t j = tiled ? tiled_index(x, y, z, nbx, nby) : i;
+        dst[j] = H(lbm::Storage<ST>::load(src[i], k));
+    }
 }
 
 // dst (device layout, global order) <- src (one field of nodes, given order/type)
@@ -93,18 +120,21 @@ __global__ void scatter_out_kernel(D *dst, const S *src, int nx, int ny, int nz,
     }
 }
 
-__global__ void reduce_kernel(const float *m, size_t N, double *acc, unsigned long long *bad)
+template <typename ST>
+__global__ void reduce_kernel(const ST *m, size_t N, double *acc, unsigned long long *bad)
 {
+    using S = lbm::Storage<ST>;
     double mass = 0.0, ke = 0.0;
     unsigned long long nb = 0;
     for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x) {
-        const double rho = double(m[i]) + 1.0;
-        const double u = double(m[N + i]) / 3.0, v = double(m[2 * N + i]) / 3.0, w = double(m[3 * N + i]) / 3.0;
+        const double rho = double(S::load(m[i], 0)) + 1.0;
+        const double u = double(S::load(m[N + i], 1)) / 3.0, v = double(S::load(m[2 * N + i], 2)) / 3.0,
+                     w = double(S::load(m[3 * N + i], 3)) / 3.0;
         mass += rho;
         ke += 0.5 * rho * (u * u + v * v + w * w);
 #pragma unroll
         for (int f = 0; f < 10; f++)
-            nb += !isfinite(m[f * N + i]);
+            nb += !isfinite(S::load(m[f * N + i], f));
     }
     for (int o = 16; o > 0; o >>= 1) {
         mass += __shfl_down_sync(0xffffffffu, mass, o);
@@ -141,82 +171,18 @@ __global__ void reduce_kernel(const float *m, size_t N, double *acc, unsigned lo
 // --------------------------------------------------------- kernel table
 using lbm::StepParams;
 
-struct TileCfg {
-    int tx, ty, stages;
-};
+using lbm::Launcher;
+using lbm::Variant;
+using lbm::kVariants;
 
-template <int Q, int TX, int TY, int NS, bool FO, typename MeanT, bool MON, int NPB, int MINB>
-void *kernel_fn()
+bool pick_launcher(int Q, int tx, int ty, int stages, int npb, int storage, bool fo, int mean_bits, Launcher &out)
 {
-    return reinterpret_cast<void *>(&lbm::step_kernel<Q, TX, TY, NS, FO, MeanT, MON, NPB, MINB>);
-}
-
-struct Launcher {
-    void *fn = nullptr;      // plain step
-    void *fn_mon = nullptr;  // step that also accumulates the per-step monitor sums
-    size_t smem = 0;
-    int tx = 0, ty = 0, stages = 0, pop_buffers = 2;
-};
-
-template <int Q, int TX, int TY, int NS, int NPB = 2, int MINB = 2>
-Launcher pick_fo(bool fo, int mean_bits)
-{
-    Launcher l;
-    l.tx = TX;
-    l.ty = TY;
-    l.stages = NS;
-    l.pop_buffers = NPB;
-    l.smem = lbm::SmemLayout<Q, TX, TY, NS, NPB>::bytes;
-    if (!fo) {
-        l.fn = kernel_fn<Q, TX, TY, NS, false, float, false, NPB, MINB>();
-        l.fn_mon = kernel_fn<Q, TX, TY, NS, false, float, true, NPB, MINB>();
-    } else if (mean_bits == 64) {
-        l.fn = kernel_fn<Q, TX, TY, NS, true, double, false, NPB, MINB>();
-        l.fn_mon = kernel_fn<Q, TX, TY, NS, true, double, true, NPB, MINB>();
-    } else {
-        l.fn = kernel_fn<Q, TX, TY, NS, true, float, false, NPB, MINB>();
-        l.fn_mon = kernel_fn<Q, TX, TY, NS, true, float, true, NPB, MINB>();
-    }
-    return l;
-}
-
-// Available tile shapes.  The first entry per lattice is the default for
-// large meshes; narrower tiles serve meshes whose nx is not a multiple of 32.
-// Every compiled kernel variant: (lattice, tile x, tile y, TMA stages,
-// population-plane code).  Population-plane code 1 = one plane, 3 CTAs/SM;
-// 2 = two planes, 2 CTAs/SM; 4 = one plane, 4 CTAs/SM.
-struct Variant {
-    int Q, tx, ty, stages, npb;
-};
-const Variant kVariants[] = {{19, 32, 8, 2, 1}, {19, 32, 8, 3, 1}, {19, 32, 8, 3, 2}, {19, 32, 8, 2, 2},
-                             {19, 32, 8, 2, 4}, {19, 16, 8, 2, 1}, {19, 8, 8, 2, 1},  {27, 32, 8, 2, 1},
-                             {27, 32, 8, 2, 2}, {27, 16, 8, 2, 1}, {27, 8, 8, 2, 1}};
-
-bool pick_launcher(int Q, int tx, int ty, int stages, int npb, bool fo, int mean_bits, Launcher &out)
-{
-#define LBM_TRY(QQ, TXX, TYY, NSS, NPB, MINB)                                    \
-    if (Q == QQ && tx == TXX && ty == TYY && stages == NSS && npb == NPB) {      \
-        out = pick_fo<QQ, TXX, TYY, NSS, NPB, MINB>(fo, mean_bits);              \
-        return true;                                                             \
-    }
-    // (lattice, tile x, tile y, TMA stages, population planes, min CTAs/SM)
-    LBM_TRY(19, 32, 8, 2, 1, 3)
-    LBM_TRY(19, 32, 8, 3, 1, 3)
-    LBM_TRY(19, 32, 8, 3, 2, 2)
-    LBM_TRY(19, 32, 8, 2, 2, 2)
-    if (Q == 19 && tx == 32 && ty == 8 && stages == 2 && npb == 4) {  // 1 plane, 4 CTAs/SM (experimental)
-        out = pick_fo<19, 32, 8, 2, 1, 4>(fo, mean_bits);
-        out.pop_buffers = 4;
-        return true;
-    }
-    LBM_TRY(19, 16, 8, 2, 1, 3)
-    LBM_TRY(19, 8, 8, 2, 1, 3)
-    LBM_TRY(27, 32, 8, 2, 1, 3)
-    LBM_TRY(27, 32, 8, 2, 2, 2)
-    LBM_TRY(27, 16, 8, 2, 1, 3)
-    LBM_TRY(27, 8, 8, 2, 1, 3)
-#undef LBM_TRY
-    return false;
+    if (storage == 1)
+        return lbm::pick_f16(Q, tx, ty, stages, npb, fo, mean_bits, out);
+    if (storage == 2)
+        return lbm::pick_bf16(Q, tx, ty, stages, npb, fo, mean_bits, out);
+    return Q == 19 ? lbm::pick_q19_f32(tx, ty, stages, npb, fo, mean_bits, out)
+                   : lbm::pick_q27_f32(tx, ty, stages, npb, fo, mean_bits, out);
 }
 
 // Default tiling for a mesh: widest tile whose width divides nx, z-chunks
@@ -259,7 +225,9 @@ struct lbm_handle {
     int Q = 19;
     size_t N = 0;
     cudaStream_t stream = nullptr;
-    float *m[2] = {nullptr, nullptr};
+    void *m[2] = {nullptr, nullptr};  // moment fields in the storage format
+    int storage = 0;                   // 0 FP32, 1 FP16, 2 BF16
+    size_t esz = 4;                    // bytes per stored moment value
     int cur = 0;
     CUtensorMap tmap[2];
     // function objects
@@ -296,12 +264,16 @@ lbm_status make_tmap(lbm_handle *h, int which)
     if (!enc)
         return fail(LBM_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
     const auto &c = h->cfg;
-    const int XPAD = 4;
+    const int XPAD = h->storage ? lbm::Storage<__half>::XPAD : lbm::Storage<float>::XPAD;
+    const cuuint64_t e = h->esz;
     cuuint64_t dims[4] = {cuuint64_t(c.nx), cuuint64_t(c.ny), cuuint64_t(c.nz), 10};
-    cuuint64_t strides[3] = {cuuint64_t(c.nx) * 4, cuuint64_t(c.nx) * c.ny * 4, cuuint64_t(h->N) * 4};
+    cuuint64_t strides[3] = {cuuint64_t(c.nx) * e, cuuint64_t(c.nx) * c.ny * e, cuuint64_t(h->N) * e};
     cuuint32_t box[4] = {cuuint32_t(h->launcher.tx + 2 * XPAD), cuuint32_t(h->launcher.ty + 2), 1, 10};
     cuuint32_t estr[4] = {1, 1, 1, 1};
-    CUresult r = enc(&h->tmap[which], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->m[which], dims, strides, box, estr,
+    const CUtensorMapDataType dt = h->storage == 1   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                   : h->storage == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                     : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    CUresult r = enc(&h->tmap[which], dt, 4, h->m[which], dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS)
@@ -365,9 +337,11 @@ dim3 grid_1d(size_t N)
 template <typename MeanT>
 lbm_status launch_step(lbm_handle *h, bool monitored = false)
 {
+    // the parameter block has the same layout for every storage type (the
+    // output is a pointer); it is filled once here as the FP32 instance
     StepParams<MeanT> p{};
     const int nxt = h->cur ^ 1;
-    p.out = h->m[nxt];
+    p.out = static_cast<float *>(h->m[nxt]);
     p.mon = h->mon;
     p.nx = int(h->cfg.nx);
     p.ny = int(h->cfg.ny);
@@ -469,6 +443,8 @@ lbm_status lbm_create(const lbm_config *cfg, lbm_handle **out)
         return fail(LBM_ERR_ARG, "mean_bits must be 32 or 64");
     if (c.function_objects & ~0x1Fu)
         return fail(LBM_ERR_ARG, "unknown function object bits");
+    if (c.storage < 0 || c.storage > 2)
+        return fail(LBM_ERR_ARG, "storage must be LBM_STORAGE_F32, LBM_STORAGE_F16 or LBM_STORAGE_BF16");
 
     int ndev = 0;
     LBM_CUDA(cudaGetDeviceCount(&ndev));
@@ -481,6 +457,8 @@ lbm_status lbm_create(const lbm_config *cfg, lbm_handle **out)
     h->Q = c.lattice;
     h->N = size_t(c.nx) * c.ny * c.nz;
     h->t = c.start_step;
+    h->storage = c.storage;
+    h->esz = c.storage ? 2 : 4;
 
     // relaxation constants in float, as the reference (latticeMesh.cuh:177-201)
     const float nu = c.u_inf * static_cast<float>(c.nx - 1) / c.Re;
@@ -497,7 +475,9 @@ lbm_status lbm_create(const lbm_config *cfg, lbm_handle **out)
     if (c.stages) st = c.stages;
     const bool fo = c.function_objects != 0;
     const int npb = c.pop_buffers ? c.pop_buffers : 1;
-    if (!pick_launcher(h->Q, tx, ty, st, npb, fo, c.mean_bits, h->launcher)) {
+    if (h->storage && tx == 8)
+        tx = 16;
+    if (!pick_launcher(h->Q, tx, ty, st, npb, h->storage, fo, c.mean_bits, h->launcher)) {
         delete h;
         return fail(LBM_ERR_ARG, "unsupported tile configuration");
     }
@@ -514,7 +494,7 @@ lbm_status lbm_create(const lbm_config *cfg, lbm_handle **out)
     LBM_CUDA(cudaEventCreate(&h->ev0));
     LBM_CUDA(cudaEventCreate(&h->ev1));
     for (int b = 0; b < 2; b++)
-        if ((s = dev_alloc(h, &h->m[b], 10 * h->N)) != LBM_OK)
+        if ((s = dev_alloc(h, reinterpret_cast<char **>(&h->m[b]), 10 * h->N * h->esz)) != LBM_OK)
             return cleanup_fail(s);
     const size_t msz = c.mean_bits == 64 ? 8 : 4;
     if (c.function_objects & LBM_FO_S)
@@ -531,7 +511,7 @@ lbm_status lbm_create(const lbm_config *cfg, lbm_handle **out)
     if ((s = dev_alloc(h, &h->red, 4)) != LBM_OK) return cleanup_fail(s);
     if ((s = dev_alloc(h, &h->mon, 1)) != LBM_OK) return cleanup_fail(s);
     for (int b = 0; b < 2; b++) {
-        cudaMemsetAsync(h->m[b], 0, 10 * h->N * 4, h->stream);
+        cudaMemsetAsync(h->m[b], 0, 10 * h->N * h->esz, h->stream);
     }
     if (h->S) cudaMemsetAsync(h->S, 0, 6 * h->N * 4, h->stream);
     if (h->k) cudaMemsetAsync(h->k, 0, h->N * 4, h->stream);
@@ -558,7 +538,7 @@ lbm_status lbm_destroy(lbm_handle *h)
     cudaSetDevice(h->cfg.device);
     if (h->stream)
         cudaStreamSynchronize(h->stream);
-    for (void *p : {static_cast<void *>(h->m[0]), static_cast<void *>(h->m[1]), static_cast<void *>(h->S),
+    for (void *p : {h->m[0], h->m[1], static_cast<void *>(h->S),
                     static_cast<void *>(h->k), h->SMean, h->kMean, h->momentsMean, static_cast<void *>(h->err),
                     static_cast<void *>(h->red), static_cast<void *>(h->mon), h->scratch})
         if (p)
@@ -580,8 +560,14 @@ lbm_status lbm_init_regions(lbm_handle *h, const float region[70])
     if (s != LBM_OK)
         return s;
     LBM_CUDA(cudaMemcpyAsync(h->scratch, region, 70 * sizeof(float), cudaMemcpyHostToDevice, h->stream));
-    init_regions_kernel<<<grid_1d(h->N), 256, 0, h->stream>>>(h->m[h->cur], int(h->cfg.nx), int(h->cfg.ny),
-                                                               int(h->cfg.nz), static_cast<float *>(h->scratch));
+    const int nx = int(h->cfg.nx), ny = int(h->cfg.ny), nz = int(h->cfg.nz);
+    const float *rg = static_cast<float *>(h->scratch);
+    if (h->storage == 1)
+        init_regions_kernel<<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<__half *>(h->m[h->cur]), nx, ny, nz, rg);
+    else if (h->storage == 2)
+        init_regions_kernel<<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<__nv_bfloat16 *>(h->m[h->cur]), nx, ny, nz, rg);
+    else
+        init_regions_kernel<<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<float *>(h->m[h->cur]), nx, ny, nz, rg);
     LBM_CUDA(cudaGetLastError());
     h->launches += 1;
     const size_t msz = h->cfg.mean_bits == 64 ? 8 : 4;
@@ -620,16 +606,37 @@ lbm_status lbm_write_fields(lbm_handle *h, lbm_field_set set, const void *host, 
         const char *src = static_cast<const char *>(host) + size_t(v) * h->N * hsz;
         LBM_CUDA(cudaMemcpyAsync(h->scratch, src, h->N * hsz, cudaMemcpyHostToDevice, h->stream));
         const int nx = int(h->cfg.nx), ny = int(h->cfg.ny), nz = int(h->cfg.nz);
-        if (dtype == LBM_F64) {
+        const dim3 g = grid_1d(h->N);
+        if (set == LBM_FIELDS_MOMENTS) {
+            // moments go through the storage format (FP32 / FP16 / BF16)
+            char *dst = static_cast<char *>(dptr) + size_t(v) * h->N * h->esz;
+            const void *sc = h->scratch;
+            if (h->storage == 1) {
+                if (dtype == LBM_F64)
+                    moment_in_kernel<<<g, 256, 0, h->stream>>>(reinterpret_cast<__half *>(dst), static_cast<const double *>(sc), v, nx, ny, nz, tiled);
+                else
+                    moment_in_kernel<<<g, 256, 0, h->stream>>>(reinterpret_cast<__half *>(dst), static_cast<const float *>(sc), v, nx, ny, nz, tiled);
+            } else if (h->storage == 2) {
+                if (dtype == LBM_F64)
+                    moment_in_kernel<<<g, 256, 0, h->stream>>>(reinterpret_cast<__nv_bfloat16 *>(dst), static_cast<const double *>(sc), v, nx, ny, nz, tiled);
+                else
+                    moment_in_kernel<<<g, 256, 0, h->stream>>>(reinterpret_cast<__nv_bfloat16 *>(dst), static_cast<const float *>(sc), v, nx, ny, nz, tiled);
+            } else {
+                if (dtype == LBM_F64)
+                    moment_in_kernel<<<g, 256, 0, h->stream>>>(reinterpret_cast<float *>(dst), static_cast<const double *>(sc), v, nx, ny, nz, tiled);
+                else
+                    moment_in_kernel<<<g, 256, 0, h->stream>>>(reinterpret_cast<float *>(dst), static_cast<const float *>(sc), v, nx, ny, nz, tiled);
+            }
+        } else if (dtype == LBM_F64) {
             if (is_double)
-                gather_in_kernel<double, double><<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<double *>(dptr) + v * h->N, static_cast<const double *>(h->scratch), nx, ny, nz, tiled);
+                gather_in_kernel<double, double><<<g, 256, 0, h->stream>>>(static_cast<double *>(dptr) + v * h->N, static_cast<const double *>(h->scratch), nx, ny, nz, tiled);
             else
-                gather_in_kernel<double, float><<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<float *>(dptr) + v * h->N, static_cast<const double *>(h->scratch), nx, ny, nz, tiled);
+                gather_in_kernel<double, float><<<g, 256, 0, h->stream>>>(static_cast<float *>(dptr) + v * h->N, static_cast<const double *>(h->scratch), nx, ny, nz, tiled);
         } else {
             if (is_double)
-                gather_in_kernel<float, double><<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<double *>(dptr) + v * h->N, static_cast<const float *>(h->scratch), nx, ny, nz, tiled);
+                gather_in_kernel<float, double><<<g, 256, 0, h->stream>>>(static_cast<double *>(dptr) + v * h->N, static_cast<const float *>(h->scratch), nx, ny, nz, tiled);
             else
-                gather_in_kernel<float, float><<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<float *>(dptr) + v * h->N, static_cast<const float *>(h->scratch), nx, ny, nz, tiled);
+                gather_in_kernel<float, float><<<g, 256, 0, h->stream>>>(static_cast<float *>(dptr) + v * h->N, static_cast<const float *>(h->scratch), nx, ny, nz, tiled);
         }
         LBM_CUDA(cudaGetLastError());
         h->launches += 1;
@@ -654,12 +661,14 @@ lbm_status lbm_read_fields(lbm_handle *h, lbm_field_set set, void *host, size_t 
     if (s != LBM_OK)
         return s;
     const size_t hsz = dtype == LBM_F64 ? 8 : 4;
-    const size_t dsz = is_double ? 8 : 4;
+    const bool moments = set == LBM_FIELDS_MOMENTS;
+    const size_t dsz = moments ? h->esz : (is_double ? 8 : 4);
     const int tiled = order == LBM_ORDER_TILED;
-    const bool direct = !tiled && hsz == dsz;
+    const bool direct = !tiled && hsz == dsz && (!moments || h->storage == 0);
     if (!direct && (s = ensure_scratch(h, h->N * hsz)) != LBM_OK)
         return s;
     const int nx = int(h->cfg.nx), ny = int(h->cfg.ny), nz = int(h->cfg.nz);
+    const dim3 g = grid_1d(h->N);
     for (int v = 0; v < nv; v++) {
         char *dst = static_cast<char *>(host) + size_t(v) * h->N * hsz;
         const char *src = static_cast<const char *>(dptr) + size_t(v) * h->N * dsz;
@@ -667,16 +676,34 @@ lbm_status lbm_read_fields(lbm_handle *h, lbm_field_set set, void *host, size_t 
             LBM_CUDA(cudaMemcpyAsync(dst, src, h->N * hsz, cudaMemcpyDeviceToHost, h->stream));
             continue;
         }
-        if (dtype == LBM_F64) {
+        void *sc = h->scratch;
+        if (moments) {
+            if (h->storage == 1) {
+                if (dtype == LBM_F64)
+                    moment_out_kernel<<<g, 256, 0, h->stream>>>(static_cast<double *>(sc), reinterpret_cast<const __half *>(src), v, nx, ny, nz, tiled);
+                else
+                    moment_out_kernel<<<g, 256, 0, h->stream>>>(static_cast<float *>(sc), reinterpret_cast<const __half *>(src), v, nx, ny, nz, tiled);
+            } else if (h->storage == 2) {
+                if (dtype == LBM_F64)
+                    moment_out_kernel<<<g, 256, 0, h->stream>>>(static_cast<double *>(sc), reinterpret_cast<const __nv_bfloat16 *>(src), v, nx, ny, nz, tiled);
+                else
+                    moment_out_kernel<<<g, 256, 0, h->stream>>>(static_cast<float *>(sc), reinterpret_cast<const __nv_bfloat16 *>(src), v, nx, ny, nz, tiled);
+            } else {
+                if (dtype == LBM_F64)
+                    moment_out_kernel<<<g, 256, 0, h->stream>>>(static_cast<double *>(sc), reinterpret_cast<const float *>(src), v, nx, ny, nz, tiled);
+                else
+                    moment_out_kernel<<<g, 256, 0, h->stream>>>(static_cast<float *>(sc), reinterpret_cast<const float *>(src), v, nx, ny, nz, tiled);
+            }
+        } else if (dtype == LBM_F64) {
             if (is_double)
-                scatter_out_kernel<double, double><<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<double *>(h->scratch), reinterpret_cast<const double *>(src), nx, ny, nz, tiled);
+                scatter_out_kernel<double, double><<<g, 256, 0, h->stream>>>(static_cast<double *>(sc), reinterpret_cast<const double *>(src), nx, ny, nz, tiled);
             else
-                scatter_out_kernel<float, double><<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<double *>(h->scratch), reinterpret_cast<const float *>(src), nx, ny, nz, tiled);
+                scatter_out_kernel<float, double><<<g, 256, 0, h->stream>>>(static_cast<double *>(sc), reinterpret_cast<const float *>(src), nx, ny, nz, tiled);
         } else {
             if (is_double)
-                scatter_out_kernel<double, float><<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<float *>(h->scratch), reinterpret_cast<const double *>(src), nx, ny, nz, tiled);
+                scatter_out_kernel<double, float><<<g, 256, 0, h->stream>>>(static_cast<float *>(sc), reinterpret_cast<const double *>(src), nx, ny, nz, tiled);
             else
-                scatter_out_kernel<float, float><<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<float *>(h->scratch), reinterpret_cast<const float *>(src), nx, ny, nz, tiled);
+                scatter_out_kernel<float, float><<<g, 256, 0, h->stream>>>(static_cast<float *>(sc), reinterpret_cast<const float *>(src), nx, ny, nz, tiled);
         }
         LBM_CUDA(cudaGetLastError());
         h->launches += 1;
@@ -746,8 +773,14 @@ lbm_status lbm_reduce(lbm_handle *h, double out[3])
         return fail(LBM_ERR_ARG, "null argument");
     LBM_CUDA(cudaSetDevice(h->cfg.device));
     LBM_CUDA(cudaMemsetAsync(h->red, 0, 4 * sizeof(double), h->stream));
-    reduce_kernel<<<grid_1d(h->N), 256, 0, h->stream>>>(h->m[h->cur], h->N, h->red,
-                                                         reinterpret_cast<unsigned long long *>(h->red + 2));
+    auto *dbad = reinterpret_cast<unsigned long long *>(h->red + 2);
+    if (h->storage == 1)
+        reduce_kernel<<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<const __half *>(h->m[h->cur]), h->N, h->red, dbad);
+    else if (h->storage == 2)
+        reduce_kernel<<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<const __nv_bfloat16 *>(h->m[h->cur]), h->N,
+                                                             h->red, dbad);
+    else
+        reduce_kernel<<<grid_1d(h->N), 256, 0, h->stream>>>(static_cast<const float *>(h->m[h->cur]), h->N, h->red, dbad);
     LBM_CUDA(cudaGetLastError());
     h->launches += 1;
     double r[3];
@@ -900,7 +933,7 @@ void save_tune_entry(const TuneEntry &e)
 lbm_status apply_variant(lbm_handle *h, int tx, int ty, int stages, int npb, int zc)
 {
     Launcher l;
-    if (!pick_launcher(h->Q, tx, ty, stages, npb, h->cfg.function_objects != 0, h->cfg.mean_bits, l))
+    if (!pick_launcher(h->Q, tx, ty, stages, npb, h->storage, h->cfg.function_objects != 0, h->cfg.mean_bits, l))
         return fail(LBM_ERR_ARG, "unsupported tile configuration");
     for (void *fn : {l.fn, l.fn_mon})
         LBM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(l.smem)));
@@ -942,7 +975,7 @@ lbm_status lbm_autotune(lbm_handle *h, int32_t trial_steps, lbm_tuning *out)
     }
     // back up the state the trials will advance
     const size_t msz = h->cfg.mean_bits == 64 ? 8 : 4;
-    std::vector<std::pair<void *, size_t>> live = {{h->m[h->cur], 10 * h->N * 4}};
+    std::vector<std::pair<void *, size_t>> live = {{h->m[h->cur], 10 * h->N * h->esz}};
     if (h->S) live.push_back({h->S, 6 * h->N * 4});
     if (h->k) live.push_back({h->k, h->N * 4});
     if (h->SMean) live.push_back({h->SMean, 6 * h->N * msz});
@@ -977,7 +1010,7 @@ lbm_status lbm_autotune(lbm_handle *h, int32_t trial_steps, lbm_tuning *out)
     int tried = 0;
     const int zcs[] = {8, 16, 32, 64};
     for (const Variant &v : kVariants) {
-        if (v.Q != h->Q || v.tx > h->cfg.nx || v.ty > h->cfg.ny)
+        if (v.Q != h->Q || v.storage != h->storage || v.tx > h->cfg.nx || v.ty > h->cfg.ny)
             continue;
         for (int zc : zcs) {
             if (zc > h->cfg.nz)

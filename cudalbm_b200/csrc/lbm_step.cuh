@@ -23,11 +23,47 @@
 #pragma once
 
 #include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "lbm_core.cuh"
 
 namespace lbm {
+
+// ------------------------------------------------------------ storage
+// How the 10 moment fields are held in HBM.  FP32 stores the reference's
+// values as they are.  The 16-bit formats store (value * scale[field]) with
+// power-of-two scales (exact to apply and undo) that bring typical cavity
+// magnitudes -- rho-1 ~ 1e-3, 3u ~ 0.1, 4.5 m_aa and 9 m_ab ~ 1e-2 -- near 1,
+// away from the fp16 subnormal range; arithmetic stays FP32.  XPAD is the
+// left padding of a TMA box so that its x start is 16-byte aligned.
+template <typename ST>
+struct Storage;
+
+template <>
+struct Storage<float> {
+    static constexpr int BYTES = 4, XPAD = 4;
+    __host__ __device__ static constexpr float scale(int) { return 1.0f; }
+    __device__ static float load(float v, int) { return v; }
+    __device__ static float store(float v, int) { return v; }
+};
+
+template <>
+struct Storage<__half> {
+    static constexpr int BYTES = 2, XPAD = 8;
+    __host__ __device__ static constexpr float scale(int k) { return (k >= 1 && k <= 3) ? 8.0f : 64.0f; }
+    __device__ static float load(__half v, int k) { return __half2float(v) * (1.0f / scale(k)); }
+    __device__ static __half store(float v, int k) { return __float2half_rn(v * scale(k)); }
+};
+
+template <>
+struct Storage<__nv_bfloat16> {
+    static constexpr int BYTES = 2, XPAD = 8;
+    __host__ __device__ static constexpr float scale(int) { return 1.0f; }
+    __device__ static float load(__nv_bfloat16 v, int) { return __bfloat162float(v); }
+    __device__ static __nv_bfloat16 store(float v, int) { return __float2bfloat16_rn(v); }
+};
 
 // ------------------------------------------------------------------ PTX
 __device__ __forceinline__ unsigned smem_u32(const void *p)
@@ -116,9 +152,9 @@ struct MonitorSlot {
     unsigned long long nonfinite;  // nodes with a NaN/Inf among their 10 stored moments
 };
 
-template <typename MeanT>
+template <typename MeanT, typename ST = float>
 struct StepParams {
-    float *out;        // [10][N] moments after the step
+    ST *out;           // [10][N] moments after the step
     MonitorSlot *mon;  // per-step sums (monitored kernels only)
     int nx, ny, nz;
     int zc;            // z-planes per CTA
@@ -128,13 +164,13 @@ struct StepParams {
     uint64_t timeout_ns;
 };
 
-template <int TX, int TY>
+template <int TX, int TY, typename ST = float>
 struct TileGeom {
-    static constexpr int XPAD = 4;             // TMA box starts 4 nodes left (16 B alignment)
-    static constexpr int TXP = TX + 2 * XPAD;  // staged row length
-    static constexpr int RY = TY + 2;          // staged rows (ring included)
-    static constexpr int PLANE_FLOATS = 10 * RY * TXP;
-    static constexpr int PLANE_BYTES = PLANE_FLOATS * 4;
+    static constexpr int XPAD = Storage<ST>::XPAD;  // TMA box starts XPAD nodes left (16 B alignment)
+    static constexpr int TXP = TX + 2 * XPAD;       // staged row length
+    static constexpr int RY = TY + 2;               // staged rows (ring included)
+    static constexpr int PLANE_FLOATS = 10 * RY * TXP;  // elements of one staged plane
+    static constexpr int PLANE_BYTES = PLANE_FLOATS * Storage<ST>::BYTES;
     static constexpr int PX = TX + 2, PY = TY + 2;  // population plane incl. ring
     static constexpr int RING = 2 * (TX + 2) + 2 * TY;
     static_assert(PLANE_BYTES % 128 == 0, "stage size must keep 128 B alignment");
@@ -142,9 +178,9 @@ struct TileGeom {
 
 // NPB population planes: 2 lets consecutive planes overlap with one barrier
 // per plane; 1 saves shared memory (more CTAs per SM) at a second barrier.
-template <int Q, int TX, int TY, int NSTAGE, int NPB = 2>
+template <int Q, int TX, int TY, int NSTAGE, int NPB = 2, typename ST = float>
 struct SmemLayout {
-    using G = TileGeom<TX, TY>;
+    using G = TileGeom<TX, TY, ST>;
     static constexpr int NXY = XY<Q>::N;
     static constexpr size_t bar_off = 0;
     static constexpr size_t stage_off = 128;
@@ -175,14 +211,14 @@ __device__ __forceinline__ void static_for(F &&f)
 
 // Reconstruct the x-y movers of ring node (rx, ry) that point into the tile
 // (those with the given sign of cx or cy) and store them into pop plane pb.
-template <int Q, int TX, int TY, int AXIS, int SIGN>
-__device__ __forceinline__ void ring_pops(const float *sm, float *pb, int rx, int ry)
+template <int Q, int TX, int TY, int AXIS, int SIGN, typename ST>
+__device__ __forceinline__ void ring_pops(const ST *sm, float *pb, int rx, int ry)
 {
-    using G = TileGeom<TX, TY>;
+    using G = TileGeom<TX, TY, ST>;
     float m[10];
 #pragma unroll
     for (int k = 0; k < 10; k++)
-        m[k] = sm[(k * G::RY + ry + 1) * G::TXP + rx + G::XPAD];
+        m[k] = Storage<ST>::load(sm[(k * G::RY + ry + 1) * G::TXP + rx + G::XPAD], k);
     m[0] = m[0] + 1.0f;
     const RecPre r = rec_pre<Q>(m);
     static_for<0, XY<Q>::N>([&](auto s) {
@@ -194,17 +230,19 @@ __device__ __forceinline__ void ring_pops(const float *sm, float *pb, int rx, in
 }
 
 // ---------------------------------------------------------------- kernel
-template <int Q, int TX, int TY, int NSTAGE, bool FO, typename MeanT, bool MON = false, int NPB = 2, int MINB = 2>
-__global__ void __launch_bounds__(TX *TY, MINB) step_kernel(const __grid_constant__ CUtensorMap tmap_in, const StepParams<MeanT> p)
+template <int Q, int TX, int TY, int NSTAGE, bool FO, typename MeanT, bool MON = false, int NPB = 2, int MINB = 2,
+          typename ST = float>
+__global__ void __launch_bounds__(TX *TY, MINB)
+    step_kernel(const __grid_constant__ CUtensorMap tmap_in, const StepParams<MeanT, ST> p)
 {
-    using G = TileGeom<TX, TY>;
-    using L = SmemLayout<Q, TX, TY, NSTAGE, NPB>;
+    using G = TileGeom<TX, TY, ST>;
+    using L = SmemLayout<Q, TX, TY, NSTAGE, NPB, ST>;
     using ZG = ZGroups<Q>;
     constexpr int NXY = XY<Q>::N;
 
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
-    float *stages = reinterpret_cast<float *>(smem + L::stage_off);
+    ST *stages = reinterpret_cast<ST *>(smem + L::stage_off);
     float *pops = reinterpret_cast<float *>(smem + L::pop_off);
     __shared__ int s_abort;
 
@@ -243,7 +281,7 @@ __global__ void __launch_bounds__(TX *TY, MINB) step_kernel(const __grid_constan
         const int pz = z0 - 1 + i;  // plane being received
         const int stage = i % NSTAGE;
         const unsigned parity = (i / NSTAGE) & 1;
-        float *sm = stages + stage * G::PLANE_FLOATS;
+        ST *sm = stages + stage * G::PLANE_FLOATS;
         float *pb = pops + (NPB == 2 ? (i & 1) : 0) * L::pop_floats;
 
         // running means of the node updated in this iteration (plane pz-1),
@@ -275,7 +313,7 @@ __global__ void __launch_bounds__(TX *TY, MINB) step_kernel(const __grid_constan
             float m[10];
 #pragma unroll
             for (int k = 0; k < 10; k++)
-                m[k] = sm[(k * G::RY + ty + 1) * G::TXP + tx + G::XPAD];
+                m[k] = Storage<ST>::load(sm[(k * G::RY + ty + 1) * G::TXP + tx + G::XPAD], k);
             m[0] = m[0] + 1.0f;
             const RecPre r = rec_pre<Q>(m);
             static_for<0, NXY>([&](auto s) {
@@ -290,14 +328,14 @@ __global__ void __launch_bounds__(TX *TY, MINB) step_kernel(const __grid_constan
         if (lin < G::RING) {
             int r = lin;
             if (r < TX + 2) {
-                ring_pops<Q, TX, TY, 1, +1>(sm, pb, r - 1, -1);
+                ring_pops<Q, TX, TY, 1, +1, ST>(sm, pb, r - 1, -1);
             } else if ((r -= TX + 2) < TX + 2) {
-                ring_pops<Q, TX, TY, 1, -1>(sm, pb, r - 1, TY);
+                ring_pops<Q, TX, TY, 1, -1, ST>(sm, pb, r - 1, TY);
             } else if ((r -= TX + 2) < TY) {
-                ring_pops<Q, TX, TY, 0, +1>(sm, pb, -1, r);
+                ring_pops<Q, TX, TY, 0, +1, ST>(sm, pb, -1, r);
             } else {
                 r -= TY;
-                ring_pops<Q, TX, TY, 0, -1>(sm, pb, TX, r);
+                ring_pops<Q, TX, TY, 0, -1, ST>(sm, pb, TX, r);
             }
         }
         __syncthreads();
@@ -332,11 +370,11 @@ __global__ void __launch_bounds__(TX *TY, MINB) step_kernel(const __grid_constan
                 const unsigned type = node_type(x, y, zu, p.nx, p.ny, p.nz);
                 float m[10];
                 node_update<Q>(f, type, p.rx, m);
-                float *o = p.out + iu;
-                o[0] = m[0] - 1.0f;
+                ST *o = p.out + iu;
+                o[0] = Storage<ST>::store(m[0] - 1.0f, 0);
 #pragma unroll
                 for (int k = 1; k < 10; k++)
-                    o[k * N] = m[k];
+                    o[k * N] = Storage<ST>::store(m[k], k);
                 if constexpr (MON) {
                     mon_mass += double(m[0]);
                     mon_ke += double(m[0] * ((m[1] * m[1] + m[2] * m[2]) + m[3] * m[3]));

@@ -1,0 +1,17 @@
+// variants_f16.cu -- step-kernel instantiations (see lbm_variants.cuh).
+#include "lbm_step.cuh"
+#include "lbm_variants.cuh"
+
+namespace lbm {
+
+bool pick_f16(int Q, int tx, int ty, int stages, int npb, bool fo, int mean_bits, Launcher &out)
+{
+    LBM_VARIANT(19, 32, 8, 2, 1, 1, 3, __half)
+    LBM_VARIANT(19, 32, 8, 3, 1, 1, 3, __half)
+    LBM_VARIANT(19, 16, 8, 2, 1, 1, 3, __half)
+    LBM_VARIANT(27, 32, 8, 2, 1, 1, 3, __half)
+    LBM_VARIANT(27, 16, 8, 2, 1, 1, 3, __half)
+    return false;
+}
+
+}  // namespace lbm

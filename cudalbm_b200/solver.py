@@ -31,7 +31,8 @@ class Cavity:
 
     def __init__(self, lattice: int, nx: int, ny: int, nz: int, Re: float, u_inf: float,
                  function_objects: Iterable[str] = (), mean_bits: int = 32, device: int = 0,
-                 start_step: int = 0, tile: Optional[tuple] = None, z_chunk: int = 0, pop_buffers: int = 0):
+                 start_step: int = 0, tile: Optional[tuple] = None, z_chunk: int = 0, pop_buffers: int = 0,
+                 storage: str = "f32"):
         L = _lib.lib()
         cfg = _lib.Config()
         L.lbm_config_default(ctypes.byref(cfg))
@@ -51,6 +52,8 @@ class Cavity:
                 cfg.stages = int(tile[2])
         cfg.z_chunk = int(z_chunk)
         cfg.pop_buffers = int(pop_buffers)
+        cfg.storage = _lib.STORAGE[storage]
+        self.storage = storage
         self.cfg = cfg
         self.shape = (nz, ny, nx)
         self.mean_bits = mean_bits

@@ -80,7 +80,14 @@ typedef struct lbm_config {
     /* kernel tiling; 0 = autotuned choice for this size class */
     int32_t tile_x, tile_y, z_chunk, stages;
     int32_t pop_buffers;      /* shared-memory population planes: 2 (one barrier per plane) or 1 */
+    int32_t storage;          /* LBM_STORAGE_*: how the 10 moment fields are held in device memory */
 } lbm_config;
+
+/* Moment storage formats.  Arithmetic is FP32 for all of them; the 16-bit
+ * formats hold each field times a power of two (rho-1 and the second-order
+ * moments x64, 3u x8 for FP16; x1 for BF16) and convert to the reference's
+ * FP32 values at every host transfer. */
+enum { LBM_STORAGE_F32 = 0, LBM_STORAGE_F16 = 1, LBM_STORAGE_BF16 = 2 };
 
 typedef struct lbm_handle lbm_handle;
 
