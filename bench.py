@@ -74,6 +74,10 @@ WORKLOADS = {
                         storage="f16", desc="D3Q19 lid-driven cavity 768^3, Re=1000, u_lid=0.05, FP16 moment storage"),
     "q19_768_bf16": dict(lattice=19, n=(768, 768, 768), Re=1000.0, u=0.05, fo=(), mean_bits=32, b_alg=55,
                          storage="bf16", desc="D3Q19 lid-driven cavity 768^3, Re=1000, u_lid=0.05, BF16 moment storage"),
+    "batch64_q19": dict(kind="batch", lattice=19, n_cav=64, seed=0, Re=None, u=0.05, fo=(), b_alg=110,
+                        desc="64 D3Q19 cubic lid-driven cavities in one persistent launch per step (CUDA graph): "
+                             "MT19937-64 seed 0 draws edges from {32,48,64,96,128} and Re from U[100,2000], "
+                             "u_lid=0.05, FP32"),
     "q27_256_fo64": dict(lattice=27, n=(256, 256, 256), Re=1000.0, u=0.05, fo=("S", "SMean", "k", "kMean"),
                          mean_bits=64, b_alg=274,
                          desc="D3Q27 lid-driven cavity 256^3, Re=1000, function objects with FP64 means"),
@@ -318,23 +322,133 @@ def run_ours(args, w):
     return line
 
 
-# ------------------------------------------------------- reference arm
-def run_reference(args, w):
+# ------------------------------------------------------ batched arm
+def run_batch(args, w):
+    """Aggregate MLUPS of many cavities advanced by one persistent launch per
+    step, beside the same cavities stepped by one plain launch each, one after
+    another on the same stream (the single-cavity path, each size class with
+    its own autotuned kernel)."""
+    import numpy as np
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return None
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        return {"impl": "ours", "unavailable": "the batched workload is measured on one GPU"} if rank == 0 else None
+
+    from cudalbm_b200 import _lib, casefiles
+    from cudalbm_b200.solver import Batch
+
+    specs = casefiles.random_cavities(w["n_cav"], seed=w["seed"], lattice=w["lattice"], u_lid=w["u"])
+    nodes = sum(c["nx"] * c["ny"] * c["nz"] for c in specs)
+    b = Batch(specs, device=local)
+    b.init_regions()
+    tuning = None if args.no_autotune else b.autotune(args.tune_steps)
+    b.step(args.warmup)
+    b.synchronize()
+
+    # ---- device-timed batched loop (value)
+    sampler = ClockSampler(physical_gpu_index(local))
+    sampler.start()
+    launches0 = b.info()["kernel_launches"]
+    b.step(args.steps)
+    b.synchronize()
+    info = b.info()
+    clocks = sampler.stop()
+    ms = info["last_step_ms"]
+    ms_step = ms / args.steps
+    value = nodes * args.steps / (ms / 1e3) / 1e6
+    launches = info["kernel_launches"] - launches0
+
+    # ---- the same cavities, one plain launch each per step (wall clock)
+    for c in b.cavities:
+        c.autotune(args.tune_steps)
+    seq_steps = max(3, min(args.steps, 200))
+    for c in b.cavities:
+        c.step(1)
+    b.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(seq_steps):
+        for c in b.cavities:
+            c.step(1)
+    b.synchronize()
+    seq = nodes * seq_steps / (time.perf_counter() - t0) / 1e6
+    t0 = time.perf_counter()
+    b.step(seq_steps)
+    b.synchronize()
+    batch_wall = nodes * seq_steps / (time.perf_counter() - t0) / 1e6
+
+    # ---- end to end through the C ABI with pinned host buffers
+    states = [_lib.PinnedArray((10, c.shape[0], c.shape[1], c.shape[2]), np.float32) for c in b.cavities]
+    for c, st in zip(b.cavities, states):
+        c.read("moments", out=st.array)
+    t0 = time.perf_counter()
+    for c, st in zip(b.cavities, states):
+        c.write(st.array)
+    b.step(args.steps)
+    for c, st in zip(b.cavities, states):
+        c.read("moments", out=st.array)
+    e2e_s = time.perf_counter() - t0
+    e2e = nodes * args.steps / e2e_s / 1e6
+    state_bytes = sum(st.array.nbytes for st in states)
+    bad = sum(int(c.reduce()["nonfinite"]) for c in b.cavities)
+    b.close()
+
+    peak, peak_kind = hbm_peak()
+    achieved = w["b_alg"] * nodes / (ms_step / 1e3) / 1e9
+    edges = {}
+    for c in specs:
+        edges[c["nx"]] = edges.get(c["nx"], 0) + 1
+    line = {
+        "metric": METRIC,
+        "value": round(value, 2),
+        "unit": "MLUPS",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_step, 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic: 64 lid-driven cavity initial states (seeded sizes and Reynolds numbers)",
+        "config": {"workload": w["desc"], "lattice": f"D3Q{w['lattice']}", "cavities": len(specs), "nodes": nodes,
+                   "edges": {str(k): v for k, v in sorted(edges.items())}, "parallelism": "1 GPU",
+                   "l2": "inputs larger than L2 (moment buffers %.2f GB vs 126 MB L2); no flush" % (80 * nodes / 1e9)},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None, "bytes_per_node_alg": w["b_alg"],
+                     "peak_kind": f"of {peak_kind}"},
+        "e2e": {"value": round(e2e, 2), "unit": "MLUPS", "h2d_bytes_per_step": round(state_bytes / args.steps),
+                "d2h_bytes_per_step": round(state_bytes / args.steps),
+                "what": "lbm_write_fields of every cavity (pinned h2d) + lbm_batch_step(K) + lbm_read_fields of "
+                        "every cavity's moments"},
+        "sequential": {"value": round(seq, 2), "unit": "MLUPS", "steps": seq_steps,
+                       "what": "each step = 64 plain launches (one per cavity, autotuned per size class), one after "
+                               "another on one stream; wall clock",
+                       "batched_same_clock": round(batch_wall, 2),
+                       "speedup": round(batch_wall / seq, 3)},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "check": {"nonfinite": bad},
+        "kernel": {"tile": [info["tile_x"], info["tile_y"]], "stages": info["stages"],
+                   "pop_buffers": info["pop_buffers"], "grid": info["grid"], "items": info["items"],
+                   "graph_launches_timed": args.steps // 2, "autotuned": tuning},
+    }
+    if not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(dict(lattice=19, n=(64, 64, 64), Re=specs[0]["Re"], u=w["u"], fo=(),
+                                                     desc="one 64^3 D3Q19 cavity of the batch"))
+        except Exception as exc:
+            line["cpu_baseline"] = {"value": None, "error": repr(exc)}
+    return line
+
+
+# ------------------------------------------------------- reference arm
+def reference_step_time(exe, spec, W, K, local):
+    """Seconds per step of the reference executable on one case, from its
+    per-step 'Time:' lines (K steps after W); (dt, clocks, error)."""
     from cudalbm_b200 import casefiles
 
-    exe = os.path.join(ROOT, "oracle", "_ref", f"momentBasedD3Q{w['lattice']}")
-    if not os.path.exists(exe):
-        return {"impl": "reference", "unavailable": f"{exe} not built (make -f oracle/Makefile.ref needs the "
-                                                    "reference sources)"}
-    nx, ny, nz = w["n"]
-    nodes = nx * ny * nz
-    W, K = args.warmup, args.steps
-    spec = casefiles.CaseSpec(nx=nx, ny=ny, nz=nz, Re=w["Re"], u_inf=w["u"], n_steps=W + K + 1,
-                              save_interval=W + K + 10, info_interval=1, function_objects=w["fo"])
-    local = int(os.environ.get("LOCAL_RANK", "0"))
     with tempfile.TemporaryDirectory() as case:
         casefiles.write_case(case, spec)
         sampler = ClockSampler(physical_gpu_index(local))
@@ -355,8 +469,55 @@ def run_reference(args, w):
                     clocks = sampler.stop()
         rc = proc.wait()
     if rc != 0 or W not in stamps or W + K not in stamps:
-        return {"impl": "reference", "unavailable": f"reference exited {rc}: {''.join(tail)[-300:]!r}"}
-    dt = (stamps[W + K] - stamps[W]) / K
+        return None, None, f"reference exited {rc}: {''.join(tail)[-300:]!r}"
+    return (stamps[W + K] - stamps[W]) / K, clocks, None
+
+
+def run_reference(args, w):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    from cudalbm_b200 import casefiles
+
+    exe = os.path.join(ROOT, "oracle", "_ref", f"momentBasedD3Q{w['lattice']}")
+    if not os.path.exists(exe):
+        return {"impl": "reference", "unavailable": f"{exe} not built (make -f oracle/Makefile.ref needs the "
+                                                    "reference sources)"}
+    W, K = args.warmup, args.steps
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if w.get("kind") == "batch":
+        # the reference runs one cavity per process: time each size class once
+        # and charge every cavity of the batch its class's step time
+        cavs = casefiles.random_cavities(w["n_cav"], seed=w["seed"], lattice=w["lattice"])
+        per_edge, clocks = {}, None
+        for e in sorted({c["nx"] for c in cavs}):
+            c0 = next(c for c in cavs if c["nx"] == e)
+            spec = casefiles.CaseSpec(nx=e, ny=e, nz=e, Re=c0["Re"], u_inf=w["u"], n_steps=W + K + 1,
+                                      save_interval=W + K + 10, info_interval=1)
+            dt, clk, err = reference_step_time(exe, spec, W, K, local)
+            if err:
+                return {"impl": "reference", "unavailable": err}
+            per_edge[e] = dt
+            clocks = clk or clocks
+        nodes = sum(c["nx"] ** 3 for c in cavs)
+        dt = sum(per_edge[c["nx"]] for c in cavs)
+        cfg = {"workload": w["desc"], "lattice": f"D3Q{w['lattice']}", "cavities": len(cavs), "nodes": nodes,
+               "parallelism": "1 GPU", "seconds_per_step_by_edge": {str(k): v for k, v in per_edge.items()}}
+        sample = ("the reference's own executable run once per size class (one cavity per process, as it "
+                  f"supports), {K} steps after {W} each, per-step times summed over the 64 cavities")
+    else:
+        nx, ny, nz = w["n"]
+        nodes = nx * ny * nz
+        spec = casefiles.CaseSpec(nx=nx, ny=ny, nz=nz, Re=w["Re"], u_inf=w["u"], n_steps=W + K + 1,
+                                  save_interval=W + K + 10, info_interval=1, function_objects=w["fo"])
+        dt, clocks, err = reference_step_time(exe, spec, W, K, local)
+        if err:
+            return {"impl": "reference", "unavailable": err}
+        cfg = {"workload": w["desc"], "lattice": f"D3Q{w['lattice']}", "nx": nx, "ny": ny, "nz": nz,
+               "Re": w["Re"], "u_lid": w["u"], "function_objects": list(w["fo"]), "parallelism": "1 GPU"}
+        sample = (f"the reference's own executable (oracle/_ref/momentBasedD3Q{w['lattice']}, built from its "
+                  f"sources for sm_100a) on the B200 -- its only implementation is CUDA; {K} steps after {W}, timed "
+                  "by its per-step 'Time:' lines (wall clock, the reference synchronises the device every step)")
     value = nodes / dt / 1e6
     return {
         "impl": "reference",
@@ -371,14 +532,10 @@ def run_reference(args, w):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
-        "data": "synthetic: the same lid-driven cavity case directory",
-        "config": {"workload": w["desc"], "lattice": f"D3Q{w['lattice']}", "nx": nx, "ny": ny, "nz": nz,
-                   "Re": w["Re"], "u_lid": w["u"], "function_objects": list(w["fo"]), "parallelism": "1 GPU"},
+        "data": "synthetic: the same lid-driven cavity case directories",
+        "config": cfg,
         "cpu_baseline": {"value": round(value, 2), "unit": "MLUPS", "cores": 1, "kind": "reference",
-                         "sample": f"the reference's own executable (oracle/_ref/momentBasedD3Q{w['lattice']}, built "
-                                   "from its sources for sm_100a) on the B200 -- its only implementation is CUDA; "
-                                   f"{K} steps after {W}, timed by its per-step 'Time:' lines (wall clock, the "
-                                   "reference synchronises the device every step)"},
+                         "sample": sample},
         "e2e": {"value": round(value, 2), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "clocks": clocks,
     }
@@ -403,7 +560,12 @@ def main():
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     w = WORKLOADS[args.workload]
-    line = run_reference(args, w) if args.impl == "reference" else run_ours(args, w)
+    if args.impl == "reference":
+        line = run_reference(args, w)
+    elif w.get("kind") == "batch":
+        line = run_batch(args, w)
+    else:
+        line = run_ours(args, w)
     if line is not None:
         print(json.dumps(line), flush=True)
 

@@ -30,7 +30,9 @@ F32, F64 = 0, 1
 EXPORTS = ("lbm_config_default", "lbm_create", "lbm_destroy", "lbm_init_regions", "lbm_write_fields",
            "lbm_read_fields", "lbm_step", "lbm_synchronize", "lbm_reduce", "lbm_get_info", "lbm_last_error",
            "lbm_status_string", "lbm_field_set_vars", "lbm_host_alloc", "lbm_host_free", "lbm_case_read",
-           "lbm_lbmbin_write", "lbm_reduce_moments_noalloc", "lbm_step_monitored", "lbm_autotune")
+           "lbm_lbmbin_write", "lbm_reduce_moments_noalloc", "lbm_step_monitored", "lbm_autotune",
+           "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_cavity", "lbm_batch_step", "lbm_batch_synchronize",
+           "lbm_batch_autotune", "lbm_batch_get_info", "lbm_batch_configure")
 
 
 class Config(ctypes.Structure):
@@ -56,6 +58,21 @@ class Tuning(ctypes.Structure):
     _fields_ = [("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32), ("z_chunk", ctypes.c_int32),
                 ("stages", ctypes.c_int32), ("pop_buffers", ctypes.c_int32), ("ms_per_step", ctypes.c_double),
                 ("candidates", ctypes.c_int32), ("from_cache", ctypes.c_int32)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("cavities", ctypes.c_int32), ("items", ctypes.c_int32), ("grid", ctypes.c_int32),
+                ("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32), ("stages", ctypes.c_int32),
+                ("pop_buffers", ctypes.c_int32), ("persistent", ctypes.c_int32), ("nodes", ctypes.c_int64),
+                ("step", ctypes.c_int64),
+                ("device_bytes", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint64),
+                ("graph_launches", ctypes.c_uint64), ("last_step_ms", ctypes.c_double)]
+
+
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32), ("stages", ctypes.c_int32),
+                ("pop_buffers", ctypes.c_int32), ("persistent", ctypes.c_int32), ("size_classes", ctypes.c_int32),
+                ("candidates", ctypes.c_int32), ("ms_per_step", ctypes.c_double)]
 
 
 class Case(ctypes.Structure):
@@ -108,11 +125,21 @@ def lib() -> ctypes.CDLL:
         L.lbm_reduce_moments_noalloc.argtypes = [vp, u64, ctypes.POINTER(ctypes.c_double), vp]
         L.lbm_step_monitored.argtypes = [vp, u64, vp]
         L.lbm_autotune.argtypes = [vp, i32, ctypes.POINTER(Tuning)]
+        L.lbm_batch_create.argtypes = [ctypes.POINTER(Config), i32, ctypes.POINTER(vp)]
+        L.lbm_batch_destroy.argtypes = [vp]
+        L.lbm_batch_cavity.argtypes = [vp, i32, ctypes.POINTER(vp)]
+        L.lbm_batch_step.argtypes = [vp, u64]
+        L.lbm_batch_synchronize.argtypes = [vp]
+        L.lbm_batch_autotune.argtypes = [vp, i32, ctypes.POINTER(BatchTuning)]
+        L.lbm_batch_get_info.argtypes = [vp, ctypes.POINTER(BatchInfo)]
+        L.lbm_batch_configure.argtypes = [vp, ctypes.POINTER(BatchTuning)]
         L.lbm_lbmbin_write.argtypes = [ctypes.c_char_p, u64, u64, u64, i32, ctypes.POINTER(ctypes.c_char_p), vp, u64,
                                        i32]
         for name in ("lbm_create", "lbm_destroy", "lbm_init_regions", "lbm_write_fields", "lbm_read_fields",
                      "lbm_step", "lbm_synchronize", "lbm_reduce", "lbm_get_info", "lbm_host_alloc", "lbm_host_free",
-                     "lbm_case_read", "lbm_lbmbin_write", "lbm_reduce_moments_noalloc", "lbm_step_monitored", "lbm_autotune"):
+                     "lbm_case_read", "lbm_lbmbin_write", "lbm_reduce_moments_noalloc", "lbm_step_monitored", "lbm_autotune",
+                     "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_cavity", "lbm_batch_step",
+                     "lbm_batch_synchronize", "lbm_batch_autotune", "lbm_batch_get_info", "lbm_batch_configure"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib

@@ -203,3 +203,62 @@ def relaxation(u_inf: float, Re: float, nx: int):
     tau = f32(0.5) + f32(3.0) * nu
     omega = f32(1.0) / tau
     return tau, omega, f32(1.0) - omega, omega * f32(0.5)
+
+
+# ------------------------------------------------------ batched workloads
+class MT19937_64:
+    """The 64-bit Mersenne Twister (Matsumoto & Nishimura 2004; the engine of
+    C++'s std::mt19937_64), so that seeded workloads are reproducible in any
+    host language without a library."""
+
+    _N, _M = 312, 156
+    _A = 0xB5026F5AA96619E9
+    _UPPER, _LOWER = 0xFFFFFFFF80000000, 0x7FFFFFFF
+    _MASK = (1 << 64) - 1
+
+    def __init__(self, seed: int):
+        mt = [seed & self._MASK]
+        for i in range(1, self._N):
+            prev = mt[-1]
+            mt.append((6364136223846793005 * (prev ^ (prev >> 62)) + i) & self._MASK)
+        self._mt, self._i = mt, self._N
+
+    def _twist(self) -> None:
+        mt, n, m = self._mt, self._N, self._M
+        for i in range(n):
+            x = (mt[i] & self._UPPER) | (mt[(i + 1) % n] & self._LOWER)
+            xa = (x >> 1) ^ (self._A if x & 1 else 0)
+            mt[i] = mt[(i + m) % n] ^ xa
+        self._i = 0
+
+    def next(self) -> int:
+        if self._i >= self._N:
+            self._twist()
+        y = self._mt[self._i]
+        self._i += 1
+        y ^= (y >> 29) & 0x5555555555555555
+        y ^= (y << 17) & 0x71D67FFFEDA60000
+        y ^= (y << 37) & 0xFFF7EEE000000000
+        y ^= y >> 43
+        return y & self._MASK
+
+
+BATCH_EDGES = (32, 48, 64, 96, 128)
+
+
+def random_cavities(n: int = 64, seed: int = 0, edges=BATCH_EDGES, re_range=(100.0, 2000.0), u_lid: float = 0.05,
+                    lattice: int = 19):
+    """Cubic lid-driven cavities of uneven size and Reynolds number.
+
+    MT19937-64 seeded with `seed`; for each cavity in turn, one draw x picks
+    the edge edges[x % len(edges)] and the next draw y gives
+    Re = lo + (hi - lo) * (y >> 11) / 2^53.  Returns a list of dicts with the
+    keys of solver.Cavity."""
+    g = MT19937_64(seed)
+    lo, hi = re_range
+    out = []
+    for _ in range(n):
+        e = int(edges[g.next() % len(edges)])
+        re = lo + (hi - lo) * ((g.next() >> 11) * 2.0 ** -53)
+        out.append(dict(lattice=lattice, nx=e, ny=e, nz=e, Re=float(re), u_inf=u_lid))
+    return out

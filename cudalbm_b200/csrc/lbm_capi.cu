@@ -22,6 +22,7 @@
 
 #include "casefile.hpp"
 #include "lbm_b200.h"
+#include "lbm_handle.hpp"
 #include "lbm_step.cuh"
 #include "lbmbin.hpp"
 #include "lbm_variants.cuh"
@@ -200,9 +201,7 @@ void default_tiling(int Q, int64_t nx, int64_t ny, int64_t nz, int &tx, int &ty,
     zc = int(c);
 }
 
-using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+using lbm::EncodeTiledFn;
 
 EncodeTiledFn get_encode()
 {
@@ -219,34 +218,6 @@ EncodeTiledFn get_encode()
 }
 
 }  // namespace
-
-struct lbm_handle {
-    lbm_config cfg{};
-    int Q = 19;
-    size_t N = 0;
-    cudaStream_t stream = nullptr;
-    void *m[2] = {nullptr, nullptr};  // moment fields in the storage format
-    int storage = 0;                   // 0 FP32, 1 FP16, 2 BF16
-    size_t esz = 4;                    // bytes per stored moment value
-    int cur = 0;
-    CUtensorMap tmap[2];
-    // function objects
-    float *S = nullptr, *k = nullptr;
-    void *SMean = nullptr, *kMean = nullptr, *momentsMean = nullptr;
-    unsigned *err = nullptr;
-    double *red = nullptr;
-    void *scratch = nullptr;
-    size_t scratch_bytes = 0;
-    float tau = 0, omega = 0, t_omega = 0, omega_d2 = 0;
-    int64_t t = 0;
-    Launcher launcher;
-    int zc = 0;
-    uint64_t device_bytes = 0;
-    uint64_t launches = 0;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    bool timed = false;
-    lbm::MonitorSlot *mon = nullptr;  // one slot, reused by every monitored step
-};
 
 namespace {
 
@@ -364,7 +335,7 @@ lbm_status launch_step(lbm_handle *h, bool monitored = false)
     p.fo.sd.d_ij = 2.0f * 9.0f * h->tau;
     p.fo.sd.r_ii = 1.0f / p.fo.sd.d_ii;
     p.fo.sd.r_ij = 1.0f / p.fo.sd.d_ij;
-    p.err = h->err;
+    p.fault = h->err;
     p.timeout_ns = 2000000000ull;
     const dim3 block(h->launcher.tx, h->launcher.ty);
     const dim3 grid(unsigned((h->cfg.nx + h->launcher.tx - 1) / h->launcher.tx),
@@ -386,6 +357,42 @@ namespace lbm {
 lbm_status record_error(lbm_status s, const std::string &msg)
 {
     return fail(s, msg);
+}
+
+EncodeTiledFn encode_tiled() { return get_encode(); }
+
+lbm_status check_fault(const StepFault &f, const char *who)
+{
+    if (!(f.flags & ERR_TMA_TIMEOUT))
+        return LBM_OK;
+    std::string msg = std::string(who) + " timed out waiting for a TMA copy";
+    if (f.recorded == 1) {
+        char buf[256];
+        std::snprintf(buf, sizeof(buf),
+                      " (block %d,%d,%d item %d mesh %d plane %d seq %u slot %u parity %u mbarrier 0x%016llx)",
+                      f.block[0], f.block[1], f.block[2], f.item, f.mesh, f.plane, f.seq, f.slot, f.parity, f.barrier);
+        msg += buf;
+    }
+    return fail(LBM_ERR_TIMEOUT, msg);
+}
+
+void destroy_handle(lbm_handle *h)
+{
+    if (!h)
+        return;
+    cudaSetDevice(h->cfg.device);
+    if (h->stream)
+        cudaStreamSynchronize(h->stream);
+    for (void *p : {h->m[0], h->m[1], static_cast<void *>(h->S), static_cast<void *>(h->k), h->SMean, h->kMean,
+                    h->momentsMean, static_cast<void *>(h->err), static_cast<void *>(h->red),
+                    static_cast<void *>(h->mon), h->scratch})
+        if (p)
+            cudaFree(p);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream && h->own_stream)
+        cudaStreamDestroy(h->stream);
+    delete h;
 }
 }  // namespace lbm
 
@@ -507,7 +514,7 @@ lbm_status lbm_create(const lbm_config *cfg, lbm_handle **out)
         if ((s = dev_alloc(h, reinterpret_cast<char **>(&h->kMean), h->N * msz)) != LBM_OK) return cleanup_fail(s);
     if (c.function_objects & LBM_FO_MOMENTSMEAN)
         if ((s = dev_alloc(h, reinterpret_cast<char **>(&h->momentsMean), 10 * h->N * msz)) != LBM_OK) return cleanup_fail(s);
-    if ((s = dev_alloc(h, &h->err, 4)) != LBM_OK) return cleanup_fail(s);
+    if ((s = dev_alloc(h, &h->err, 1)) != LBM_OK) return cleanup_fail(s);
     if ((s = dev_alloc(h, &h->red, 4)) != LBM_OK) return cleanup_fail(s);
     if ((s = dev_alloc(h, &h->mon, 1)) != LBM_OK) return cleanup_fail(s);
     for (int b = 0; b < 2; b++) {
@@ -518,7 +525,7 @@ lbm_status lbm_create(const lbm_config *cfg, lbm_handle **out)
     if (h->SMean) cudaMemsetAsync(h->SMean, 0, 6 * h->N * msz, h->stream);
     if (h->kMean) cudaMemsetAsync(h->kMean, 0, h->N * msz, h->stream);
     if (h->momentsMean) cudaMemsetAsync(h->momentsMean, 0, 10 * h->N * msz, h->stream);
-    cudaMemsetAsync(h->err, 0, 4, h->stream);
+    cudaMemsetAsync(h->err, 0, sizeof(lbm::StepFault), h->stream);
     if (cudaGetLastError() != cudaSuccess)
         return cleanup_fail(fail(LBM_ERR_CUDA, "cudaMemsetAsync failed"));
     for (int b = 0; b < 2; b++)
@@ -535,19 +542,9 @@ lbm_status lbm_destroy(lbm_handle *h)
 {
     if (!h)
         return LBM_OK;
-    cudaSetDevice(h->cfg.device);
-    if (h->stream)
-        cudaStreamSynchronize(h->stream);
-    for (void *p : {h->m[0], h->m[1], static_cast<void *>(h->S),
-                    static_cast<void *>(h->k), h->SMean, h->kMean, h->momentsMean, static_cast<void *>(h->err),
-                    static_cast<void *>(h->red), static_cast<void *>(h->mon), h->scratch})
-        if (p)
-            cudaFree(p);
-    if (h->ev0) cudaEventDestroy(h->ev0);
-    if (h->ev1) cudaEventDestroy(h->ev1);
-    if (h->stream)
-        cudaStreamDestroy(h->stream);
-    delete h;
+    if (h->batch)
+        return fail(LBM_ERR_STATE, "this cavity belongs to a batch: destroy the batch instead");
+    lbm::destroy_handle(h);
     return LBM_OK;
 }
 
@@ -760,11 +757,9 @@ lbm_status lbm_synchronize(lbm_handle *h)
         return fail(LBM_ERR_ARG, "null handle");
     LBM_CUDA(cudaSetDevice(h->cfg.device));
     LBM_CUDA(cudaStreamSynchronize(h->stream));
-    unsigned e = 0;
-    LBM_CUDA(cudaMemcpy(&e, h->err, 4, cudaMemcpyDeviceToHost));
-    if (e & lbm::ERR_TMA_TIMEOUT)
-        return fail(LBM_ERR_TIMEOUT, "a step kernel timed out waiting for a TMA copy");
-    return LBM_OK;
+    lbm::StepFault f{};
+    LBM_CUDA(cudaMemcpy(&f, h->err, sizeof(f), cudaMemcpyDeviceToHost));
+    return lbm::check_fault(f, "a step kernel");
 }
 
 lbm_status lbm_reduce(lbm_handle *h, double out[3])

@@ -1,0 +1,73 @@
+// lbm_handle.hpp -- internal: the state behind an lbm_handle, shared by the
+// translation units of the library (not installed, not part of the C ABI).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "lbm_b200.h"
+#include "lbm_step.cuh"
+#include "lbm_variants.cuh"
+
+struct lbm_batch;
+
+struct lbm_handle {
+    lbm_config cfg{};
+    int Q = 19;
+    size_t N = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = true;            // false while the handle belongs to a batch (batch stream)
+    lbm_batch *batch = nullptr;        // owning batch, if any (then lbm_destroy refuses)
+    void *m[2] = {nullptr, nullptr};  // moment fields in the storage format
+    int storage = 0;                   // 0 FP32, 1 FP16, 2 BF16
+    size_t esz = 4;                    // bytes per stored moment value
+    int cur = 0;
+    CUtensorMap tmap[2];
+    // function objects
+    float *S = nullptr, *k = nullptr;
+    void *SMean = nullptr, *kMean = nullptr, *momentsMean = nullptr;
+    lbm::StepFault *err = nullptr;    // device-side error record of the step kernels
+    double *red = nullptr;
+    void *scratch = nullptr;
+    size_t scratch_bytes = 0;
+    float tau = 0, omega = 0, t_omega = 0, omega_d2 = 0;
+    int64_t t = 0;
+    lbm::Launcher launcher;
+    int zc = 0;
+    uint64_t device_bytes = 0;
+    uint64_t launches = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool timed = false;
+    lbm::MonitorSlot *mon = nullptr;  // one slot, reused by every monitored step
+};
+
+namespace lbm {
+
+// Sets the message returned by lbm_last_error() and returns s.
+lbm_status record_error(lbm_status s, const std::string &msg);
+
+// cuTensorMapEncodeTiled from the driver (null if unavailable).
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled();
+
+// Frees a handle regardless of batch ownership (used by lbm_batch_destroy).
+void destroy_handle(lbm_handle *h);
+
+// LBM_OK, or the status and message for a device-side error record.
+lbm_status check_fault(const StepFault &f, const char *who);
+
+}  // namespace lbm
+
+#define LBM_CUDA_RETURN(call)                                                                                    \
+    do {                                                                                                         \
+        cudaError_t e_ = (call);                                                                                 \
+        if (e_ != cudaSuccess)                                                                                   \
+            return lbm::record_error(e_ == cudaErrorMemoryAllocation ? LBM_ERR_NOMEM : LBM_ERR_CUDA,            \
+                                     std::string(#call) + ": " + cudaGetErrorString(e_) + " (" +                \
+                                         std::to_string((int)e_) + ")");                                         \
+    } while (0)

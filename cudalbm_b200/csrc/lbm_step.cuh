@@ -8,7 +8,7 @@
 //   2. reconstructs the populations of its nodes (and, on the ring, only the
 //      ones that point into the tile) and writes the ones that move in x-y
 //      into a double-buffered shared-memory plane;
-//   3. after one __syncthreads, pulls f_q(x) = R_q(m(x - c_q)) for every
+//   3. after one CTA barrier, pulls f_q(x) = R_q(m(x - c_q)) for every
 //      direction: x-y movers from shared memory, pure-z movers and the rest
 //      population from registers of the previous/next plane;
 //   4. updates the plane below (whose three source planes are now complete):
@@ -70,22 +70,6 @@ __device__ __forceinline__ unsigned smem_u32(const void *p)
 {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
-__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void fence_mbar_init()
-{
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void fence_proxy_async()
-{
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
 {
     unsigned ok;
@@ -118,21 +102,68 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity
             return false;
     }
 }
-__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3, uint64_t *bar)
+// CTA-wide barrier.  Each warp first reconverges (__syncwarp), then the CTA
+// synchronises; a warp split across divergent paths when it reaches a CTA
+// barrier can be released only in part.
+__device__ __forceinline__ void cta_sync()
+{
+    __syncwarp();
+    asm volatile("barrier.sync 0;" ::: "memory");
+}
+
+// Thread-0 work as predicated instructions executed by the whole warp, so
+// that no branch splits warp 0 (every thread calls these; only those with
+// `pred` act).
+//   TMA issue: make earlier ordinary reads of the slot visible to the async
+//   proxy, arm the slot's mbarrier with the plane's bytes, start the copy.
+__device__ __forceinline__ void tma_issue_if(bool pred, void *dst, const CUtensorMap *map, int c0, int c1, int c2,
+                                             int c3, uint64_t *bar, unsigned bytes)
 {
     asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(
-            smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.u32 p, %8, 0;\n\t"
+        "@p fence.proxy.async.shared::cta;\n\t"
+        "@p mbarrier.arrive.expect_tx.shared::cta.b64 _, [%6], %7;\n\t"
+        "@p cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];\n\t}" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar)), "r"(bytes),
+        "r"(unsigned(pred))
         : "memory");
 }
-__device__ __forceinline__ void prefetch_tmap(const CUtensorMap *map)
+//   mbarrier set-up: count 1 (the arming thread), then publish the init.
+__device__ __forceinline__ void mbar_init_if(bool pred, uint64_t *bar)
 {
-    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "@p mbarrier.init.shared::cta.b64 [%0], 1;\n\t}" ::"r"(smem_u32(bar)),
+        "r"(unsigned(pred))
+        : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init_if(bool pred)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.u32 p, %0, 0;\n\t"
+        "@p fence.mbarrier_init.release.cluster;\n\t}" ::"r"(unsigned(pred))
+        : "memory");
 }
 
 // ------------------------------------------------------------- params
 enum : unsigned { ERR_TMA_TIMEOUT = 1u };
+
+// Device-side error record of the step kernels: flag bits, and where the
+// first failure happened (the first CTA to fail fills in the details).
+struct StepFault {
+    unsigned flags;              // ERR_* bits
+    unsigned recorded;           // set once the details below are valid
+    int block[3];                // blockIdx of the CTA
+    int item, mesh;              // batch work item and mesh-table row (-1 outside batches)
+    int plane;                   // plane index within the work item (0 = plane z0-1)
+    unsigned seq;                // planes the CTA had received before this one
+    unsigned slot, parity;       // stage slot waited on and the phase parity expected
+    unsigned long long barrier;  // raw 64-bit mbarrier word when the wait gave up
+};
 
 template <typename MeanT>
 struct FOPtrs {
@@ -160,7 +191,7 @@ struct StepParams {
     int zc;            // z-planes per CTA
     Relax rx;
     FOPtrs<MeanT> fo;
-    unsigned *err;
+    StepFault *fault;
     uint64_t timeout_ns;
 };
 
@@ -230,26 +261,71 @@ __device__ __forceinline__ void ring_pops(const ST *sm, float *pb, int rx, int r
 }
 
 // ---------------------------------------------------------------- kernel
-template <int Q, int TX, int TY, int NSTAGE, bool FO, typename MeanT, bool MON = false, int NPB = 2, int MINB = 2,
-          typename ST = float>
-__global__ void __launch_bounds__(TX *TY, MINB)
-    step_kernel(const __grid_constant__ CUtensorMap tmap_in, const StepParams<MeanT, ST> p)
+// Shared memory of a step CTA: mbarriers, TMA stage ring, population plane(s).
+template <typename ST>
+struct CtaSmem {
+    uint64_t *bars;
+    ST *stages;
+    float *pops;
+};
+template <int Q, int TX, int TY, int NSTAGE, int NPB, typename ST>
+__device__ __forceinline__ CtaSmem<ST> cta_smem(unsigned char *smem)
+{
+    using L = SmemLayout<Q, TX, TY, NSTAGE, NPB, ST>;
+    return {reinterpret_cast<uint64_t *>(smem + L::bar_off), reinterpret_cast<ST *>(smem + L::stage_off),
+            reinterpret_cast<float *>(smem + L::pop_off)};
+}
+
+// Per-thread monitor sums (monitored kernels only).
+struct MonAcc {
+    double mass = 0.0, ke = 0.0;
+    unsigned bad = 0;
+};
+
+static __device__ __noinline__ void record_fault(StepFault *f, unsigned flag, int item, int mesh, int plane, unsigned seq,
+                                          unsigned slot, unsigned parity, const uint64_t *bar)
+{
+    atomicOr(&f->flags, flag);
+    if (atomicCAS(&f->recorded, 0u, 2u) == 0u) {
+        f->block[0] = blockIdx.x;
+        f->block[1] = blockIdx.y;
+        f->block[2] = blockIdx.z;
+        f->item = item;
+        f->mesh = mesh;
+        f->plane = plane;
+        f->seq = seq;
+        f->slot = slot;
+        f->parity = parity;
+        f->barrier = *reinterpret_cast<const volatile unsigned long long *>(bar);
+        __threadfence();
+        atomicExch(&f->recorded, 1u);
+    }
+}
+
+// One work item: tile (bx, by) of the x-y plane, z-chunk bz of the mesh that
+// p and tmap describe.  The planes a CTA receives are numbered g0, g0+1, ...
+// across all the items it processes, so that the stage slot (g % NSTAGE), the
+// phase of its mbarrier ((g / NSTAGE) & 1) and the population plane (g & 1)
+// keep cycling from one item to the next; the mbarriers are initialised once
+// per CTA.  Returns false, uniformly across the CTA, when a TMA wait timed
+// out (the error flag is then set).
+template <int Q, int TX, int TY, int NSTAGE, bool FO, typename MeanT, bool MON, int NPB, typename ST>
+__device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepParams<MeanT, ST> &p, int bx, int by,
+                                            int bz, unsigned g0, const CtaSmem<ST> &sh, int *s_abort, MonAcc &acc,
+                                            int item = -1, int mesh = -1)
 {
     using G = TileGeom<TX, TY, ST>;
     using L = SmemLayout<Q, TX, TY, NSTAGE, NPB, ST>;
     using ZG = ZGroups<Q>;
     constexpr int NXY = XY<Q>::N;
-
-    extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::bar_off);
-    ST *stages = reinterpret_cast<ST *>(smem + L::stage_off);
-    float *pops = reinterpret_cast<float *>(smem + L::pop_off);
-    __shared__ int s_abort;
+    uint64_t *const bars = sh.bars;
+    ST *const stages = sh.stages;
+    float *const pops = sh.pops;
 
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int lin = ty * TX + tx;
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-    const int z0 = blockIdx.z * p.zc;
+    const int x0 = bx * TX, y0 = by * TY;
+    const int z0 = bz * p.zc;
     const int z1 = min(z0 + p.zc, p.nz);
     const int nplanes = z1 - z0 + 2;  // planes z0-1 .. z1
     const int x = x0 + tx, y = y0 + ty;
@@ -257,32 +333,24 @@ __global__ void __launch_bounds__(TX *TY, MINB)
     const size_t N = size_t(p.nx) * p.ny * p.nz;
     const size_t plane = size_t(p.nx) * p.ny;
 
-    if (lin == 0) {
-        prefetch_tmap(&tmap_in);
-        for (int s = 0; s < NSTAGE; s++)
-            mbar_init(&bars[s], 1);
-        fence_mbar_init();
-        s_abort = 0;
-    }
-    __syncthreads();
-    if (lin == 0) {
-        for (int s = 0; s < NSTAGE && s < nplanes; s++) {
-            mbar_expect_tx(&bars[s], G::PLANE_BYTES);
-            tma_load_4d(stages + s * G::PLANE_FLOATS, &tmap_in, x0 - G::XPAD, y0 - 1, z0 - 1 + s, 0, &bars[s]);
-        }
+    // first planes of the item (the slots were last read by ordinary loads)
+#pragma unroll
+    for (int s = 0; s < NSTAGE; s++) {
+        const unsigned slot = (g0 + s) % NSTAGE;
+        tma_issue_if(lin == 0 && s < nplanes, stages + slot * G::PLANE_FLOATS, tmap, x0 - G::XPAD, y0 - 1, z0 - 1 + s,
+                     0, &bars[slot], G::PLANE_BYTES);
     }
 
     // populations held in registers between planes
     float U2[ZG::NU], U1[ZG::NU], S1[ZG::NS];  // U(p-2), U(p-1), S(p-1)
-    double mon_mass = 0.0, mon_ke = 0.0;
-    unsigned mon_bad = 0;
 
     for (int i = 0; i < nplanes; i++) {
         const int pz = z0 - 1 + i;  // plane being received
-        const int stage = i % NSTAGE;
-        const unsigned parity = (i / NSTAGE) & 1;
+        const unsigned g = g0 + i;
+        const int stage = g % NSTAGE;
+        const unsigned parity = (g / NSTAGE) & 1;
         ST *sm = stages + stage * G::PLANE_FLOATS;
-        float *pb = pops + (NPB == 2 ? (i & 1) : 0) * L::pop_floats;
+        float *pb = pops + (NPB == 2 ? (g & 1) : 0) * L::pop_floats;
 
         // running means of the node updated in this iteration (plane pz-1),
         // loaded early so the latency hides behind the reconstruction
@@ -303,8 +371,8 @@ __global__ void __launch_bounds__(TX *TY, MINB)
         }
 
         if (!mbar_wait_bounded(&bars[stage], parity, p.timeout_ns)) {
-            atomicOr(p.err, ERR_TMA_TIMEOUT);
-            s_abort = 1;
+            record_fault(p.fault, ERR_TMA_TIMEOUT, item, mesh, i, g0 + i, stage, parity, &bars[stage]);
+            *s_abort = 1;
         }
 
         // own node: reconstruct all directions
@@ -338,16 +406,13 @@ __global__ void __launch_bounds__(TX *TY, MINB)
                 ring_pops<Q, TX, TY, 0, -1, ST>(sm, pb, TX, r);
             }
         }
-        __syncthreads();
-        if (s_abort)
-            break;
+        cta_sync();
+        if (*s_abort)
+            return false;
 
         // the stage is consumed: refill it with plane i + NSTAGE
-        if (lin == 0 && i + NSTAGE < nplanes) {
-            fence_proxy_async();
-            mbar_expect_tx(&bars[stage], G::PLANE_BYTES);
-            tma_load_4d(sm, &tmap_in, x0 - G::XPAD, y0 - 1, pz + NSTAGE, 0, &bars[stage]);
-        }
+        tma_issue_if(lin == 0 && i + NSTAGE < nplanes, sm, tmap, x0 - G::XPAD, y0 - 1, pz + NSTAGE, 0, &bars[stage],
+                     G::PLANE_BYTES);
 
         // pull the down-movers (cz = -1) that land on plane pz-1
         static_for<0, NXY>([&](auto s) {
@@ -376,10 +441,10 @@ __global__ void __launch_bounds__(TX *TY, MINB)
                 for (int k = 1; k < 10; k++)
                     o[k * N] = Storage<ST>::store(m[k], k);
                 if constexpr (MON) {
-                    mon_mass += double(m[0]);
-                    mon_ke += double(m[0] * ((m[1] * m[1] + m[2] * m[2]) + m[3] * m[3]));
+                    acc.mass += double(m[0]);
+                    acc.ke += double(m[0] * ((m[1] * m[1] + m[2] * m[2]) + m[3] * m[3]));
                     const float chk = (((m[0] + m[1]) + (m[2] + m[3])) + ((m[4] + m[5]) + (m[6] + m[7]))) + (m[8] + m[9]);
-                    mon_bad += !isfinite(chk);
+                    acc.bad += !isfinite(chk);
                 }
                 if constexpr (FO) {
                     if (p.fo.S || p.fo.SMean) {
@@ -432,44 +497,192 @@ __global__ void __launch_bounds__(TX *TY, MINB)
         for (int k = 0; k < ZG::NS; k++)
             S1[k] = S0[k];
         if constexpr (NPB == 1)
-            __syncthreads();  // the single population plane is rewritten next iteration
+            cta_sync();  // the single population plane is rewritten next iteration
     }
+    return true;
+}
 
-    if constexpr (MON) {
-        // CTA sums, then one FP64 atomic per quantity
-        for (int o = 16; o > 0; o >>= 1) {
-            mon_mass += __shfl_down_sync(0xffffffffu, mon_mass, o);
-            mon_ke += __shfl_down_sync(0xffffffffu, mon_ke, o);
-            mon_bad += __shfl_down_sync(0xffffffffu, mon_bad, o);
+// CTA sums of the monitor, then one FP64 atomic per quantity.
+template <int NT>
+__device__ __forceinline__ void monitor_flush(MonAcc a, MonitorSlot *mon, int lin)
+{
+    for (int o = 16; o > 0; o >>= 1) {
+        a.mass += __shfl_down_sync(0xffffffffu, a.mass, o);
+        a.ke += __shfl_down_sync(0xffffffffu, a.ke, o);
+        a.bad += __shfl_down_sync(0xffffffffu, a.bad, o);
+    }
+    __shared__ double s_mon[2][NT / 32];
+    __shared__ unsigned s_bad[NT / 32];
+    const int lane = lin & 31, wid = lin >> 5;
+    if (lane == 0) {
+        s_mon[0][wid] = a.mass;
+        s_mon[1][wid] = a.ke;
+        s_bad[wid] = a.bad;
+    }
+    cta_sync();
+    if (lin == 0) {
+        double m = 0.0, k = 0.0;
+        unsigned long long c = 0;
+        for (int w = 0; w < NT / 32; w++) {
+            m += s_mon[0][w];
+            k += s_mon[1][w];
+            c += s_bad[w];
         }
-        __shared__ double s_mon[2][TX * TY / 32];
-        __shared__ unsigned s_bad[TX * TY / 32];
-        const int lane = lin & 31, wid = lin >> 5;
-        if (lane == 0) {
-            s_mon[0][wid] = mon_mass;
-            s_mon[1][wid] = mon_ke;
-            s_bad[wid] = mon_bad;
-        }
-        __syncthreads();
-        if (lin == 0) {
-            double a = 0.0, b = 0.0;
-            unsigned long long c = 0;
-            for (int w = 0; w < TX * TY / 32; w++) {
-                a += s_mon[0][w];
-                b += s_mon[1][w];
-                c += s_bad[w];
+        atomicAdd(&mon->mass, m);
+        atomicAdd(&mon->rho_u2, k);
+        atomicAdd(&mon->nonfinite, c);
+    }
+}
+
+template <int NSTAGE>
+__device__ __forceinline__ void init_barriers(uint64_t *bars, bool pred)
+{
+#pragma unroll
+    for (int s = 0; s < NSTAGE; s++)
+        mbar_init_if(pred, &bars[s]);
+    fence_mbar_init_if(pred);
+}
+
+// After a timeout: give TMA copies still in flight a bounded chance to land
+// before the CTA exits (both phases are polled, each for at most 1 ms).
+template <int NSTAGE>
+__device__ __forceinline__ void drain_after_abort(uint64_t *bars)
+{
+    for (int s = 0; s < NSTAGE; s++)
+        for (unsigned ph = 0; ph < 2; ph++)
+            (void)mbar_wait_bounded(&bars[s], ph, 1000000ull);
+}
+
+// One step of one mesh: CTA (bx, by, bz) of the grid marches its work item.
+template <int Q, int TX, int TY, int NSTAGE, bool FO, typename MeanT, bool MON = false, int NPB = 2, int MINB = 2,
+          typename ST = float>
+__global__ void __launch_bounds__(TX *TY, MINB)
+    step_kernel(const __grid_constant__ CUtensorMap tmap_in, const StepParams<MeanT, ST> p)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ int s_abort;
+    const CtaSmem<ST> sh = cta_smem<Q, TX, TY, NSTAGE, NPB, ST>(smem);
+    const int lin = threadIdx.y * TX + threadIdx.x;
+    init_barriers<NSTAGE>(sh.bars, lin == 0);
+    s_abort = 0;
+    cta_sync();
+    MonAcc acc;
+    march_chunk<Q, TX, TY, NSTAGE, FO, MeanT, MON, NPB, ST>(&tmap_in, p, blockIdx.x, blockIdx.y, blockIdx.z, 0u, sh,
+                                                            &s_abort, acc);
+    if constexpr (MON)
+        monitor_flush<TX * TY>(acc, p.mon, lin);
+    if (s_abort && lin == 0)
+        drain_after_abort<NSTAGE>(sh.bars);
+}
+
+// ------------------------------------------------------------ batches
+// Many independent meshes advanced by one launch per step: a persistent grid
+// (as many CTAs as fit on the GPU at once) takes work items -- one tile and
+// z-chunk of one mesh each -- from a global counter until all are done.
+// Items are numbered mesh by mesh in the order of the mesh table, which the
+// host sorts so that the biggest items come first.
+struct BatchMesh {
+    float *m[2];          // moment buffers [10][nz][ny][nx] (FP32)
+    int nx, ny, nz, zc;   // mesh and z-planes per work item
+    int tiles_x, tiles_y; // tiles per x-y plane
+    int item_begin;       // first work item of this mesh
+    int cur;              // buffer that holds the state when flip == 0
+    Relax rx;
+};
+
+struct BatchParams {
+    const BatchMesh *mesh;   // [nmesh], item_begin ascending
+    const CUtensorMap *tmap; // [2 * nmesh]: buffer b of mesh i at 2 i + b (global memory)
+    int nmesh, items;
+    unsigned *next;          // next unclaimed work item
+    unsigned *done;          // CTAs that have finished; the last one resets both counters
+    StepFault *fault;
+    uint64_t timeout_ns;
+    int persistent;          // 1: CTAs claim items from *next; 0: one item per CTA, item = blockIdx.x
+};
+
+// Acquire a tensor map that was written to global memory by a copy from the
+// host before the launch, for use by the tensor-map proxy.  The writer is the
+// host, so the fence takes system scope.
+__device__ __forceinline__ void tmap_acquire_if(bool pred, const CUtensorMap *map)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "@p fence.proxy.tensormap::generic.acquire.sys [%0], 128;\n\t}" ::"l"(reinterpret_cast<uint64_t>(map)),
+        "r"(unsigned(pred))
+        : "memory");
+}
+
+template <int Q, int TX, int TY, int NSTAGE, int NPB, int MINB>
+__global__ void __launch_bounds__(TX *TY, MINB) batch_kernel(const BatchParams bp, const int flip)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ int s_abort, s_item;
+    const CtaSmem<float> sh = cta_smem<Q, TX, TY, NSTAGE, NPB, float>(smem);
+    const int lin = threadIdx.y * TX + threadIdx.x;
+    init_barriers<NSTAGE>(sh.bars, lin == 0);
+    s_abort = 0;
+    MonAcc acc;
+    unsigned g = 0;  // planes received so far by this CTA
+    for (int round = 0;; round++) {
+        // s_item is rewritten only after every thread has passed a barrier
+        // inside march_chunk, i.e. after all of them have read it
+        if (lin < 32) {
+            // warp 0 claims the item together (the shuffle keeps it converged)
+            unsigned v = 0;
+            if (bp.persistent) {
+                if (lin == 0)
+                    v = atomicAdd(bp.next, 1u);
+                v = __shfl_sync(0xffffffffu, v, 0);
+            } else {
+                v = round == 0 ? blockIdx.x : unsigned(bp.items);
             }
-            atomicAdd(&p.mon->mass, a);
-            atomicAdd(&p.mon->rho_u2, b);
-            atomicAdd(&p.mon->nonfinite, c);
+            if (lin == 0)
+                s_item = int(v);
         }
+        cta_sync();
+        const int item = s_item;
+        if (item >= bp.items)
+            break;
+        int lo = 0, hi = bp.nmesh - 1;  // last mesh with item_begin <= item
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (bp.mesh[mid].item_begin <= item)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const BatchMesh &bm = bp.mesh[lo];
+        const int in = bm.cur ^ flip;
+        StepParams<float, float> p{};
+        p.out = bm.m[in ^ 1];
+        p.mon = nullptr;
+        p.nx = bm.nx;
+        p.ny = bm.ny;
+        p.nz = bm.nz;
+        p.zc = bm.zc;
+        p.rx = bm.rx;
+        p.fault = bp.fault;
+        p.timeout_ns = bp.timeout_ns;
+        const int local = item - bm.item_begin;
+        const int bx = local % bm.tiles_x, rest = local / bm.tiles_x;
+        const int by = rest % bm.tiles_y, bz = rest / bm.tiles_y;
+        const CUtensorMap *map = bp.tmap + 2 * lo + in;
+        tmap_acquire_if(lin == 0, map);
+        if (!march_chunk<Q, TX, TY, NSTAGE, false, float, false, NPB, float>(map, p, bx, by, bz, g, sh, &s_abort, acc,
+                                                                            item, lo))
+            break;
+        g += unsigned(min(p.zc, p.nz - bz * p.zc) + 2);
     }
-
-    if (s_abort) {
-        // give TMA copies still in flight a bounded chance to land before exit
-        if (lin == 0)
-            for (int s = 0; s < NSTAGE; s++)
-                (void)mbar_wait_bounded(&bars[s], 0, 1000000ull);
+    if (lin == 0) {
+        if (s_abort)
+            drain_after_abort<NSTAGE>(sh.bars);
+        __threadfence();
+        if (atomicAdd(bp.done, 1u) == gridDim.x - 1) {
+            *bp.next = 0;
+            *bp.done = 0;
+        }
     }
 }
 

@@ -61,8 +61,24 @@ class Cavity:
         _lib.check(L.lbm_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
 
+    @classmethod
+    def _borrowed(cls, handle: ctypes.c_void_p, cfg, owner) -> "Cavity":
+        """View of a cavity owned by a Batch (closing it releases nothing)."""
+        self = cls.__new__(cls)
+        self.function_objects = []
+        self.storage = "f32"
+        self.cfg = cfg
+        self.shape = (int(cfg.nz), int(cfg.ny), int(cfg.nx))
+        self.mean_bits = int(cfg.mean_bits)
+        self._h = handle
+        self._owner = owner
+        return self
+
     # ------------------------------------------------------------ lifecycle
     def close(self) -> None:
+        if getattr(self, "_owner", None) is not None:
+            self._h = None
+            return
         if getattr(self, "_h", None):
             _lib.lib().lbm_destroy(self._h)
             self._h = None
@@ -136,4 +152,89 @@ class Cavity:
     def info(self) -> Dict[str, object]:
         inf = _lib.Info()
         _lib.check(_lib.lib().lbm_get_info(self._h, ctypes.byref(inf)))
+        return {f: getattr(inf, f) for f, _ in inf._fields_}
+
+
+class Batch:
+    """Many independent cavities advanced by one persistent launch per step.
+
+    ``specs`` is a sequence of dicts with the keys of ``Cavity`` (lattice, nx,
+    ny, nz, Re, u_inf, ...); all share the lattice, FP32 storage, no function
+    objects.  ``batch[i]`` is a ``Cavity`` view of cavity i for state set-up
+    and read-back.
+    """
+
+    def __init__(self, specs, device: int = 0):
+        L = _lib.lib()
+        specs = list(specs)
+        cfgs = (_lib.Config * len(specs))()
+        for c, sp in zip(cfgs, specs):
+            L.lbm_config_default(ctypes.byref(c))
+            c.lattice = int(sp.get("lattice", 19))
+            c.device = int(device)
+            c.nx, c.ny, c.nz = int(sp["nx"]), int(sp["ny"]), int(sp["nz"])
+            c.Re, c.u_inf = float(sp["Re"]), float(sp.get("u_inf", 0.05))
+            c.start_step = int(sp.get("start_step", 0))
+            c.z_chunk = int(sp.get("z_chunk", 0))
+        self.cfgs = cfgs
+        b = ctypes.c_void_p()
+        _lib.check(L.lbm_batch_create(cfgs, len(specs), ctypes.byref(b)))
+        self._b = b
+        self.cavities = []
+        for i in range(len(specs)):
+            h = ctypes.c_void_p()
+            _lib.check(L.lbm_batch_cavity(b, i, ctypes.byref(h)))
+            self.cavities.append(Cavity._borrowed(h, cfgs[i], self))
+
+    def __len__(self):
+        return len(self.cavities)
+
+    def __getitem__(self, i) -> Cavity:
+        return self.cavities[i]
+
+    def close(self) -> None:
+        if getattr(self, "_b", None):
+            for c in self.cavities:
+                c.close()
+            _lib.lib().lbm_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def init_regions(self) -> None:
+        """Lid-cavity initial state in every cavity."""
+        for c in self.cavities:
+            c.init_regions()
+
+    def step(self, n: int = 1) -> None:
+        _lib.check(_lib.lib().lbm_batch_step(self._b, int(n)))
+
+    def synchronize(self) -> None:
+        _lib.check(_lib.lib().lbm_batch_synchronize(self._b))
+
+    def autotune(self, trial_steps: int = 10) -> Dict[str, object]:
+        t = _lib.BatchTuning()
+        _lib.check(_lib.lib().lbm_batch_autotune(self._b, int(trial_steps), ctypes.byref(t)))
+        return {f: getattr(t, f) for f, _ in t._fields_}
+
+    def configure(self, tile_x: int, tile_y: int = 8, stages: int = 2, pop_buffers: int = 1,
+                  persistent: bool = True) -> None:
+        """Set the batched kernel's shape by hand (instead of autotune)."""
+        t = _lib.BatchTuning(tile_x=tile_x, tile_y=tile_y, stages=stages, pop_buffers=pop_buffers,
+                             persistent=int(bool(persistent)))
+        _lib.check(_lib.lib().lbm_batch_configure(self._b, ctypes.byref(t)))
+
+    def info(self) -> Dict[str, object]:
+        inf = _lib.BatchInfo()
+        _lib.check(_lib.lib().lbm_batch_get_info(self._b, ctypes.byref(inf)))
         return {f: getattr(inf, f) for f, _ in inf._fields_}

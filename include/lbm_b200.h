@@ -200,6 +200,73 @@ lbm_status lbm_autotune(lbm_handle *h, int32_t trial_steps, lbm_tuning *out);
  * No counterpart in the reference, which has no allocation-free entry point. */
 lbm_status lbm_reduce_moments_noalloc(const float *moments, uint64_t nodes, double out[3], void *stream);
 
+/* -------------------------------------------------------------- batches
+ * Many independent cavities advanced together.  Every step is ONE launch of a
+ * persistent kernel (as many CTAs as fit on the GPU) whose CTAs take work
+ * items -- one x-y tile and z-chunk of one cavity -- from a global counter, so
+ * small cavities no longer leave the GPU idle; lbm_batch_step replays a CUDA
+ * graph that holds two such launches.  Each cavity computes exactly the bits
+ * it computes alone.  Batches run the plain method: FP32 storage and no
+ * function objects; all cavities share the lattice and the device.
+ * No counterpart in the reference, which runs one cavity per process. */
+typedef struct lbm_batch lbm_batch;
+
+typedef struct lbm_batch_info {
+    int32_t cavities;
+    int32_t items;            /* work items per step */
+    int32_t grid;             /* CTAs of the persistent launch */
+    int32_t tile_x, tile_y, stages, pop_buffers;
+    int32_t persistent;       /* 1: persistent grid claiming items; 0: one CTA per item */
+    int64_t nodes;            /* total nodes of all cavities */
+    int64_t step;             /* batch steps taken so far */
+    uint64_t device_bytes;    /* device memory of the batch tables and all cavities */
+    uint64_t kernel_launches; /* persistent launches so far (graph nodes included) */
+    uint64_t graph_launches;  /* graph replays so far */
+    double last_step_ms;      /* device time of the last lbm_batch_step call (CUDA events) */
+} lbm_batch_info;
+
+typedef struct lbm_batch_tuning {
+    int32_t tile_x, tile_y, stages, pop_buffers; /* kernel shape chosen for the whole batch */
+    int32_t persistent;       /* 1: as many CTAs as fit, claiming work items; 0: one CTA per item */
+    int32_t size_classes;     /* distinct mesh sizes, each given its own z-chunk */
+    int32_t candidates;       /* configurations timed */
+    double ms_per_step;       /* measured device time per batch step of the choice */
+} lbm_batch_tuning;
+
+/* Create n cavities (cfgs[i] as for lbm_create; same lattice and device,
+ * storage LBM_STORAGE_F32, no function objects) and the tables of the batched
+ * kernel.  The tiling fields of the configurations are ignored (see
+ * lbm_batch_autotune). */
+lbm_status lbm_batch_create(const lbm_config *cfgs, int32_t n, lbm_batch **out);
+
+/* Release the batch and all its cavities. */
+lbm_status lbm_batch_destroy(lbm_batch *b);
+
+/* Borrowed handle of cavity i (creation order), valid until lbm_batch_destroy.
+ * Every lbm_* call on a handle works on it -- lbm_init_regions, field
+ * transfers, lbm_reduce, even lbm_step of that cavity alone -- except
+ * lbm_destroy (LBM_ERR_STATE).  The cavities share the batch's stream. */
+lbm_status lbm_batch_cavity(lbm_batch *b, int32_t i, lbm_handle **out);
+
+/* Advance every cavity n steps.  Asynchronous, like lbm_step. */
+lbm_status lbm_batch_step(lbm_batch *b, uint64_t n);
+
+/* Wait for queued work and report device-side error flags. */
+lbm_status lbm_batch_synchronize(lbm_batch *b);
+
+/* Choose the batch's kernel shape (tile, pipeline depth, population planes)
+ * by timing each on the whole batch, then each size class's z-chunk, for
+ * `trial_steps` steps per candidate; the cavities' states and step counters
+ * are restored afterwards.  Allocates a temporary copy of the states. */
+lbm_status lbm_batch_autotune(lbm_batch *b, int32_t trial_steps, lbm_batch_tuning *out);
+
+lbm_status lbm_batch_get_info(lbm_batch *b, lbm_batch_info *info);
+
+/* Set the kernel shape by hand: tile_x, tile_y, stages, pop_buffers and
+ * persistent of *shape (the other fields are ignored).  LBM_ERR_ARG if no
+ * compiled kernel has that shape. */
+lbm_status lbm_batch_configure(lbm_batch *b, const lbm_batch_tuning *shape);
+
 /* Page-locked host memory for fast transfers (cudaMallocHost); free with
  * lbm_host_free.  Replaces: the reference's pinned host::array variant
  * (src/array/hostArray.cuh:66-140). */

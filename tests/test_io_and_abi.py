@@ -94,3 +94,39 @@ def test_abi_calls_that_need_no_gpu():
     cfg.nx, cfg.lattice = 16, 15
     assert L.lbm_create(ctypes.byref(cfg), ctypes.byref(h)) == 1
     assert L.lbm_create(None, ctypes.byref(h)) == 1
+
+
+def test_batch_calls_that_need_no_gpu():
+    L = _lib.lib()
+    cfgs = (_lib.Config * 2)()
+    for c in cfgs:
+        L.lbm_config_default(ctypes.byref(c))
+    b = ctypes.c_void_p()
+    assert L.lbm_batch_create(None, 2, ctypes.byref(b)) == 1
+    assert L.lbm_batch_create(cfgs, 0, ctypes.byref(b)) == 1
+    cfgs[1].lattice = 27
+    assert L.lbm_batch_create(cfgs, 2, ctypes.byref(b)) == 1
+    assert b"share the lattice" in L.lbm_last_error()
+    cfgs[1].lattice = 19
+    cfgs[0].function_objects = _lib.FO_K
+    assert L.lbm_batch_create(cfgs, 2, ctypes.byref(b)) == 1
+    assert b"plain method" in L.lbm_last_error()
+    cfgs[0].function_objects = 0
+    cfgs[0].storage = 1
+    assert L.lbm_batch_create(cfgs, 2, ctypes.byref(b)) == 1
+    assert L.lbm_batch_destroy(None) == 0
+
+
+def test_seeded_batch_workload():
+    # MT19937-64: the C++ standard's check value (10000th draw, default seed)
+    g = casefiles.MT19937_64(5489)
+    for _ in range(9999):
+        g.next()
+    assert g.next() == 9981545732273789042
+    cav = casefiles.random_cavities(64, seed=0)
+    assert len(cav) == 64
+    assert {c["nx"] for c in cav} == set(casefiles.BATCH_EDGES)
+    assert all(c["nx"] == c["ny"] == c["nz"] for c in cav)
+    assert all(100.0 <= c["Re"] < 2000.0 for c in cav)
+    assert 35e6 < sum(c["nx"] ** 3 for c in cav) < 50e6
+    assert cav == casefiles.random_cavities(64, seed=0)
