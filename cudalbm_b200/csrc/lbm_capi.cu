@@ -1003,12 +1003,16 @@ lbm_status lbm_autotune(lbm_handle *h, int32_t trial_steps, lbm_tuning *out)
     lbm_tuning best{};
     best.ms_per_step = 1e30;
     int tried = 0;
-    const int zcs[] = {8, 16, 32, 64};
+    const int zcs[] = {2, 4, 8, 16, 32, 64};
     for (const Variant &v : kVariants) {
         if (v.Q != h->Q || v.storage != h->storage || v.tx > h->cfg.nx || v.ty > h->cfg.ny)
             continue;
+        // z-chunks below 8 only for meshes too small to fill the GPU at 8
+        // (such a chunk re-reads two planes for every 2-4 it updates)
+        const int64_t tiles = ((h->cfg.nx + v.tx - 1) / v.tx) * ((h->cfg.ny + v.ty - 1) / v.ty);
+        const bool small = tiles * ((h->cfg.nz + 7) / 8) < 4 * 148 * 3;
         for (int zc : zcs) {
-            if (zc > h->cfg.nz)
+            if (zc > h->cfg.nz || (zc < 8 && !small))
                 continue;
             lbm_status s = apply_variant(h, v.tx, v.ty, v.stages, v.npb, zc);
             if (s != LBM_OK) {
