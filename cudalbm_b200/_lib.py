@@ -32,7 +32,8 @@ EXPORTS = ("lbm_config_default", "lbm_create", "lbm_destroy", "lbm_init_regions"
            "lbm_status_string", "lbm_field_set_vars", "lbm_host_alloc", "lbm_host_free", "lbm_case_read",
            "lbm_lbmbin_write", "lbm_reduce_moments_noalloc", "lbm_step_monitored", "lbm_autotune",
            "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_cavity", "lbm_batch_step", "lbm_batch_synchronize",
-           "lbm_batch_autotune", "lbm_batch_get_info", "lbm_batch_configure")
+           "lbm_batch_autotune", "lbm_batch_get_info", "lbm_batch_configure", "lbm_cut_plane",
+           "lbm_vts_write")
 
 
 class Config(ctypes.Structure):
@@ -133,13 +134,17 @@ def lib() -> ctypes.CDLL:
         L.lbm_batch_autotune.argtypes = [vp, i32, ctypes.POINTER(BatchTuning)]
         L.lbm_batch_get_info.argtypes = [vp, ctypes.POINTER(BatchInfo)]
         L.lbm_batch_configure.argtypes = [vp, ctypes.POINTER(BatchTuning)]
+        L.lbm_cut_plane.argtypes = [vp, i32, i32, ctypes.c_float, vp, sz]
+        L.lbm_vts_write.argtypes = [ctypes.c_char_p, u64, u64, u64, ctypes.POINTER(ctypes.c_float), i32,
+                                    ctypes.POINTER(ctypes.c_char_p), vp]
         L.lbm_lbmbin_write.argtypes = [ctypes.c_char_p, u64, u64, u64, i32, ctypes.POINTER(ctypes.c_char_p), vp, u64,
                                        i32]
         for name in ("lbm_create", "lbm_destroy", "lbm_init_regions", "lbm_write_fields", "lbm_read_fields",
                      "lbm_step", "lbm_synchronize", "lbm_reduce", "lbm_get_info", "lbm_host_alloc", "lbm_host_free",
                      "lbm_case_read", "lbm_lbmbin_write", "lbm_reduce_moments_noalloc", "lbm_step_monitored", "lbm_autotune",
                      "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_cavity", "lbm_batch_step",
-                     "lbm_batch_synchronize", "lbm_batch_autotune", "lbm_batch_get_info", "lbm_batch_configure"):
+                     "lbm_batch_synchronize", "lbm_batch_autotune", "lbm_batch_get_info", "lbm_batch_configure",
+                     "lbm_cut_plane", "lbm_vts_write"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib

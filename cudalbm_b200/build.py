@@ -7,6 +7,7 @@ Outputs:
   cudalbm_b200/lib/liblbm_b200.so      C ABI of include/lbm_b200.h (sm_100a)
   cudalbm_b200/bin/momentBasedD3Q19    solver executables with the reference's
   cudalbm_b200/bin/momentBasedD3Q27    command line and case files
+  cudalbm_b200/bin/fieldConvert        .LBMBin -> VTS (whole fields or cut planes)
 """
 from __future__ import annotations
 
@@ -28,7 +29,7 @@ NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-cudart"
               "-I" + INCLUDE, "-I" + CSRC] + ARCH
 
 LIB_SOURCES = ["lbm_capi.cu", "lbm_batch.cu", "variants_q19_f32.cu", "variants_q27_f32.cu", "variants_f16.cu", "variants_bf16.cu",
-               "lbm_noalloc.cu", "casefile.cpp", "lbmbin.cpp"]
+               "lbm_noalloc.cu", "casefile.cpp", "lbmbin.cpp", "postprocess.cpp"]
 
 
 def _nvcc() -> str:
@@ -85,7 +86,8 @@ def _cxx() -> str:
 
 
 def build_executables(force: bool = False) -> list:
-    """momentBasedD3Q19 / momentBasedD3Q27: host C++ over the library."""
+    """momentBasedD3Q19 / momentBasedD3Q27 (host C++ over the library) and
+    fieldConvert."""
     out = []
     main = os.path.join(CSRC, "solver_main.cpp")
     os.makedirs(BIN, exist_ok=True)
@@ -96,6 +98,12 @@ def build_executables(force: bool = False) -> list:
             _run([_cxx(), "-std=c++17", "-O2", "-Wall", "-I" + INCLUDE, "-I" + CSRC, f"-DLBM_LATTICE={q}", main] + host +
                  ["-o", exe, "-L" + os.path.dirname(LIB), "-llbm_b200", "-Wl,-rpath,$ORIGIN/../lib"])
         out.append(exe)
+    # fieldConvert: host only (no GPU, no library)
+    exe = os.path.join(BIN, "fieldConvert")
+    srcs = [os.path.join(CSRC, s) for s in ("fieldconvert_main.cpp", "casefile.cpp", "lbmbin.cpp", "postprocess.cpp")]
+    if force or _stale(exe, _deps()):
+        _run([_cxx(), "-std=c++17", "-O2", "-Wall", "-I" + INCLUDE, "-I" + CSRC] + srcs + ["-o", exe])
+    out.append(exe)
     return out
 
 

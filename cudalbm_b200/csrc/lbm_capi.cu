@@ -25,6 +25,7 @@
 #include "lbm_handle.hpp"
 #include "lbm_step.cuh"
 #include "lbmbin.hpp"
+#include "postprocess.hpp"
 #include "lbm_variants.cuh"
 
 namespace {
@@ -118,6 +119,36 @@ __global__ void scatter_out_kernel(D *dst, const S *src, int nx, int ny, int nz,
         const int x = int(i % nx), y = int((i / nx) % ny), z = int(i / (size_t(nx) * ny));
         const size_t j = tiled ? tiled_index(x, y, z, nbx, nby) : i;
         dst[j] = D(src[i]);
+    }
+}
+
+// Cut plane normal to `axis` between node planes i0 and i1 with weight w
+// (linear interpolation, no contraction into FMA so that host and device
+// round alike); out[v][a + na*b] with (a, b) = (y, z), (x, z) or (x, y).
+template <typename T>
+__device__ __forceinline__ float plane_value(const T *src, size_t N, int v, size_t node)
+{
+    if constexpr (std::is_same_v<T, float> || std::is_same_v<T, double>)
+        return float(src[size_t(v) * N + node]);
+    else
+        return lbm::Storage<T>::load(src[size_t(v) * N + node], v);
+}
+template <typename T>
+__global__ void cut_plane_kernel(float *out, const T *src, int nvars, int nx, int ny, int nz, int axis, int i0, int i1,
+                                 float w)
+{
+    const size_t N = size_t(nx) * ny * nz;
+    const int na = axis == 0 ? ny : nx, nb = axis == 2 ? ny : nz;
+    const size_t per = size_t(na) * nb;
+    for (size_t j = blockIdx.x * size_t(blockDim.x) + threadIdx.x; j < per * nvars; j += size_t(gridDim.x) * blockDim.x) {
+        const int v = int(j / per);
+        const int a = int(j % per % na), b = int(j % per / na);
+        auto node = [&](int i) {
+            const int x = axis == 0 ? i : a, y = axis == 0 ? a : (axis == 1 ? i : b), z = axis == 2 ? i : b;
+            return size_t(x) + size_t(nx) * (size_t(y) + size_t(ny) * z);
+        };
+        const float f0 = plane_value(src, N, v, node(i0)), f1 = plane_value(src, N, v, node(i1));
+        out[j] = __fadd_rn(__fmul_rn(1.0f - w, f0), __fmul_rn(w, f1));
     }
 }
 
@@ -838,6 +869,69 @@ lbm_status lbm_lbmbin_write(const char *path, uint64_t nx, uint64_t ny, uint64_t
     } catch (const std::exception &e) {
         return fail(LBM_ERR_IO, e.what());
     }
+    return LBM_OK;
+}
+
+lbm_status lbm_vts_write(const char *path, uint64_t nx, uint64_t ny, uint64_t nz, const float L[3], int32_t nvars,
+                         const char *const *names, const float *values)
+{
+    if (!path || !L || !names || !values || nvars <= 0 || nx == 0 || ny == 0 || nz == 0)
+        return fail(LBM_ERR_ARG, "null or empty argument");
+    try {
+        const uint64_t n = nx * ny * nz;
+        lbm::FieldSet f(static_cast<size_t>(nvars));
+        for (int32_t v = 0; v < nvars; v++)
+            f[v].assign(values + size_t(v) * n, values + size_t(v + 1) * n);
+        lbm::write_vts(path, f, std::vector<std::string>(names, names + nvars), nx, ny, nz, L);
+    } catch (const std::exception &e) {
+        return fail(LBM_ERR_IO, e.what());
+    }
+    return LBM_OK;
+}
+
+lbm_status lbm_cut_plane(lbm_handle *h, lbm_field_set set, int32_t axis, float position, float *host_out, size_t count)
+{
+    if (!h || !host_out)
+        return fail(LBM_ERR_ARG, "null argument");
+    if (axis < 0 || axis > 2)
+        return fail(LBM_ERR_ARG, "lbm_cut_plane: axis must be 0 (x), 1 (y) or 2 (z)");
+    const int64_t dims[3] = {h->cfg.nx, h->cfg.ny, h->cfg.nz};
+    const float index = static_cast<float>(dims[axis] - 1) * position;
+    if (!(index >= 0.0f) || index > static_cast<float>(dims[axis] - 1))
+        return fail(LBM_ERR_ARG, "lbm_cut_plane: position must lie in [0, 1]");
+    const int nv = nvars_of(set);
+    if (nv < 0)
+        return fail(LBM_ERR_ARG, "unknown field set");
+    const size_t na = size_t(axis == 0 ? h->cfg.ny : h->cfg.nx), nb = size_t(axis == 2 ? h->cfg.ny : h->cfg.nz);
+    const size_t total = size_t(nv) * na * nb;
+    if (count != total)
+        return fail(LBM_ERR_ARG, "lbm_cut_plane: count must be " + std::to_string(total));
+    LBM_CUDA(cudaSetDevice(h->cfg.device));
+    void *src = nullptr;
+    int is_double = 0;
+    lbm_status s = field_ptr(h, set, &src, &is_double);
+    if (s != LBM_OK)
+        return s;
+    if ((s = ensure_scratch(h, total * sizeof(float))) != LBM_OK)
+        return s;
+    const int i0 = int(std::floor(index)), i1 = int(std::ceil(index));
+    const float w = index - static_cast<float>(i0);
+    float *dst = static_cast<float *>(h->scratch);
+    const int nx = int(h->cfg.nx), ny = int(h->cfg.ny), nz = int(h->cfg.nz);
+    const dim3 g = grid_1d(total);
+    if (set == LBM_FIELDS_MOMENTS && h->storage == 1)
+        cut_plane_kernel<<<g, 256, 0, h->stream>>>(dst, static_cast<const __half *>(src), nv, nx, ny, nz, axis, i0, i1, w);
+    else if (set == LBM_FIELDS_MOMENTS && h->storage == 2)
+        cut_plane_kernel<<<g, 256, 0, h->stream>>>(dst, static_cast<const __nv_bfloat16 *>(src), nv, nx, ny, nz, axis, i0,
+                                                   i1, w);
+    else if (is_double)
+        cut_plane_kernel<<<g, 256, 0, h->stream>>>(dst, static_cast<const double *>(src), nv, nx, ny, nz, axis, i0, i1, w);
+    else
+        cut_plane_kernel<<<g, 256, 0, h->stream>>>(dst, static_cast<const float *>(src), nv, nx, ny, nz, axis, i0, i1, w);
+    LBM_CUDA(cudaGetLastError());
+    h->launches += 1;
+    LBM_CUDA(cudaMemcpyAsync(host_out, dst, total * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    LBM_CUDA(cudaStreamSynchronize(h->stream));
     return LBM_OK;
 }
 

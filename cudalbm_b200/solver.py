@@ -125,6 +125,18 @@ class Cavity:
     def step(self, n: int = 1) -> None:
         _lib.check(_lib.lib().lbm_step(self._h, int(n)))
 
+    def cut_plane(self, axis: int, position: float, field_set: str = "moments") -> np.ndarray:
+        """Plane normal to `axis` (0 x, 1 y, 2 z) at `position` in [0, 1]
+        between the first and last node plane, linearly interpolated on the
+        device; shape [nvars, b, a] with (a, b) = (y, z), (x, z) or (x, y)."""
+        nz, ny, nx = self.shape
+        na = ny if axis == 0 else nx
+        nb = ny if axis == 2 else nz
+        out = np.empty((NVARS[field_set], nb, na), dtype=np.float32)
+        _lib.check(_lib.lib().lbm_cut_plane(self._h, _lib.FIELD_SET[field_set], int(axis), float(position),
+                                            out.ctypes.data, out.size))
+        return out
+
     def step_monitored(self, n: int, out=None):
         """n steps, each returning (mass, rho*|u_stored|^2, nonfinite) sums
         computed by the step kernel; ``out`` is a structured array of length
@@ -153,6 +165,19 @@ class Cavity:
         inf = _lib.Info()
         _lib.check(_lib.lib().lbm_get_info(self._h, ctypes.byref(inf)))
         return {f: getattr(inf, f) for f, _ in inf._fields_}
+
+
+def write_vts(path: str, fields: np.ndarray, names: Iterable[str], lengths=(1.0, 1.0, 1.0)) -> None:
+    """VTK XML structured grid of fields [nvars, nz, ny, nx] (the file format
+    of fieldConvert -fileType vts)."""
+    fields = np.ascontiguousarray(fields, dtype=np.float32)
+    if fields.ndim == 3:  # one plane: [nvars, ny, nx]
+        fields = fields.reshape((fields.shape[0], 1) + fields.shape[1:])
+    nv, nz, ny, nx = fields.shape
+    names = [n.encode() for n in names]
+    arr = (ctypes.c_char_p * nv)(*names)
+    L = (ctypes.c_float * 3)(*lengths)
+    _lib.check(_lib.lib().lbm_vts_write(path.encode(), nx, ny, nz, L, nv, arr, fields.ctypes.data))
 
 
 class Batch:

@@ -303,6 +303,23 @@ lbm_status lbm_lbmbin_write(const char *path, uint64_t nx, uint64_t ny, uint64_t
                             const char *const *names, const float *values, uint64_t time_step,
                             int32_t time_average);
 
+/* Cut plane of a field set from the live state (fieldConvert -cutPlane,
+ * applications/fieldConvert/fieldConvert.cuh:236-326, evaluated on the
+ * device).  The plane is normal to `axis` (0 x, 1 y, 2 z) at `position` in
+ * [0, 1] between the first and the last node plane, linearly interpolated
+ * between the two bracketing node planes with weight index - floor(index)
+ * (the reference uses position - floor(index), which is right only on a
+ * node plane).  host_out receives count = nvars * (plane nodes) floats laid
+ * out [var][b][a] with (a, b) = (y, z), (x, z) or (x, y) for axis 0, 1, 2. */
+lbm_status lbm_cut_plane(lbm_handle *h, lbm_field_set set, int32_t axis, float position, float *host_out,
+                         size_t count);
+
+/* Write a VTK XML structured-grid file (fieldConvert -fileType vts,
+ * src/postProcess/VTS.cuh:68-212): `values` holds nvars*nx*ny*nz floats in
+ * [field][z][y][x] order; L = domain lengths (latticeMesh Lx, Ly, Lz). */
+lbm_status lbm_vts_write(const char *path, uint64_t nx, uint64_t ny, uint64_t nz, const float L[3], int32_t nvars,
+                         const char *const *names, const float *values);
+
 /* Message of the last failure on this thread (empty if none). */
 const char *lbm_last_error(void);
 

@@ -42,3 +42,27 @@ def max_abs(a, b):
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
     return np.max(np.abs(a - b), axis=tuple(range(1, a.ndim)))
+
+
+def read_vts(path):
+    """Minimal reader of the VTK XML structured-grid files fieldConvert writes
+    (appended raw data, UInt64 block headers): (extent, {name: values}, points)."""
+    import re
+
+    raw = open(path, "rb").read()
+    mark = raw.index(b'<AppendedData encoding="raw">_') + len(b'<AppendedData encoding="raw">_')
+    head = raw[:mark].decode()
+    extent = [int(v) for v in re.search(r'WholeExtent="([^"]+)"', head).group(1).split()]
+    arrays = re.findall(r'<DataArray type="Float32" Name="([^"]+)"(?: NumberOfComponents="3")? format="appended" '
+                        r'offset="(\d+)"/>', head)
+    out, points = {}, None
+    for name, off in arrays:
+        p = mark + int(off)
+        nbytes = int(np.frombuffer(raw[p:p + 8], dtype="<u8")[0])
+        vals = np.frombuffer(raw[p + 8:p + 8 + nbytes], dtype="<f4")
+        if name == "Coordinates":
+            points = vals.reshape(-1, 3)
+        else:
+            out[name] = vals
+    assert raw.endswith(b"</AppendedData>\n</VTKFile>\n")
+    return extent, out, points
