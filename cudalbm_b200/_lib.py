@@ -33,7 +33,9 @@ EXPORTS = ("lbm_config_default", "lbm_create", "lbm_destroy", "lbm_init_regions"
            "lbm_lbmbin_write", "lbm_reduce_moments_noalloc", "lbm_step_monitored", "lbm_autotune",
            "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_cavity", "lbm_batch_step", "lbm_batch_synchronize",
            "lbm_batch_autotune", "lbm_batch_get_info", "lbm_batch_configure", "lbm_cut_plane",
-           "lbm_vts_write")
+           "lbm_vts_write", "lbm_perturb_velocity", "lbm_filter_2to1", "lbm_trainer_create", "lbm_trainer_destroy",
+           "lbm_trainer_add", "lbm_trainer_samples", "lbm_trainer_fit", "lbm_trainer_gradient", "lbm_mlp_infer",
+           "lbm_closure_set", "lbm_closure_dtau")
 
 
 class Config(ctypes.Structure):
@@ -74,6 +76,24 @@ class BatchTuning(ctypes.Structure):
     _fields_ = [("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32), ("stages", ctypes.c_int32),
                 ("pop_buffers", ctypes.c_int32), ("persistent", ctypes.c_int32), ("size_classes", ctypes.c_int32),
                 ("candidates", ctypes.c_int32), ("ms_per_step", ctypes.c_double)]
+
+
+class MLP(ctypes.Structure):
+    _fields_ = [("w1", ctypes.c_float * 512), ("b1", ctypes.c_float * 32), ("w2", ctypes.c_float * 1024),
+                ("b2", ctypes.c_float * 32), ("w3", ctypes.c_float * 32), ("b3", ctypes.c_float),
+                ("in_mean", ctypes.c_float * 16), ("in_scale", ctypes.c_float * 16), ("in_lo", ctypes.c_float * 16),
+                ("in_hi", ctypes.c_float * 16), ("out_scale", ctypes.c_float), ("dtau_lo", ctypes.c_float),
+                ("dtau_hi", ctypes.c_float)]
+
+
+class TrainOptions(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_int32), ("batch", ctypes.c_int32), ("lr", ctypes.c_float),
+                ("dtau_lo", ctypes.c_float), ("dtau_hi", ctypes.c_float), ("seed", ctypes.c_uint64)]
+
+
+class TrainReport(ctypes.Structure):
+    _fields_ = [("samples", ctypes.c_uint64), ("steps", ctypes.c_uint64), ("loss_first", ctypes.c_double),
+                ("loss_last", ctypes.c_double), ("target_rms", ctypes.c_double)]
 
 
 class Case(ctypes.Structure):
@@ -137,6 +157,18 @@ def lib() -> ctypes.CDLL:
         L.lbm_cut_plane.argtypes = [vp, i32, i32, ctypes.c_float, vp, sz]
         L.lbm_vts_write.argtypes = [ctypes.c_char_p, u64, u64, u64, ctypes.POINTER(ctypes.c_float), i32,
                                     ctypes.POINTER(ctypes.c_char_p), vp]
+        L.lbm_perturb_velocity.argtypes = [vp, ctypes.c_float, u64]
+        L.lbm_filter_2to1.argtypes = [vp, vp]
+        L.lbm_trainer_create.argtypes = [i32, u64, ctypes.POINTER(vp)]
+        L.lbm_trainer_destroy.argtypes = [vp]
+        L.lbm_trainer_add.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.POINTER(u64)]
+        L.lbm_trainer_samples.argtypes = [vp, u64, u64, vp, vp, ctypes.POINTER(u64)]
+        L.lbm_trainer_fit.argtypes = [vp, ctypes.POINTER(TrainOptions), ctypes.POINTER(MLP), ctypes.POINTER(TrainReport)]
+        L.lbm_trainer_gradient.argtypes = [vp, ctypes.POINTER(MLP), u64, u64, ctypes.POINTER(MLP),
+                                           ctypes.POINTER(ctypes.c_double)]
+        L.lbm_mlp_infer.argtypes = [i32, ctypes.POINTER(MLP), vp, u64, vp, i32]
+        L.lbm_closure_set.argtypes = [vp, ctypes.POINTER(MLP)]
+        L.lbm_closure_dtau.argtypes = [vp, vp, sz]
         L.lbm_lbmbin_write.argtypes = [ctypes.c_char_p, u64, u64, u64, i32, ctypes.POINTER(ctypes.c_char_p), vp, u64,
                                        i32]
         for name in ("lbm_create", "lbm_destroy", "lbm_init_regions", "lbm_write_fields", "lbm_read_fields",
@@ -144,7 +176,10 @@ def lib() -> ctypes.CDLL:
                      "lbm_case_read", "lbm_lbmbin_write", "lbm_reduce_moments_noalloc", "lbm_step_monitored", "lbm_autotune",
                      "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_cavity", "lbm_batch_step",
                      "lbm_batch_synchronize", "lbm_batch_autotune", "lbm_batch_get_info", "lbm_batch_configure",
-                     "lbm_cut_plane", "lbm_vts_write"):
+                     "lbm_cut_plane", "lbm_vts_write", "lbm_perturb_velocity", "lbm_filter_2to1",
+                     "lbm_trainer_create", "lbm_trainer_destroy", "lbm_trainer_add", "lbm_trainer_samples",
+                     "lbm_trainer_fit", "lbm_trainer_gradient", "lbm_mlp_infer", "lbm_closure_set",
+                     "lbm_closure_dtau"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib

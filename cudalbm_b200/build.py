@@ -28,7 +28,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-cudart", "static",
               "-I" + INCLUDE, "-I" + CSRC] + ARCH
 
-LIB_SOURCES = ["lbm_capi.cu", "lbm_batch.cu", "variants_q19_f32.cu", "variants_q27_f32.cu", "variants_f16.cu", "variants_bf16.cu",
+LIB_SOURCES = ["lbm_capi.cu", "lbm_batch.cu", "lbm_closure.cu", "variants_q19_f32.cu", "variants_q27_f32.cu", "variants_f16.cu", "variants_bf16.cu",
                "lbm_noalloc.cu", "casefile.cpp", "lbmbin.cpp", "postprocess.cpp"]
 
 

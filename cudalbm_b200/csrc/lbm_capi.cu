@@ -23,6 +23,7 @@
 #include "casefile.hpp"
 #include "lbm_b200.h"
 #include "lbm_handle.hpp"
+#include "lbm_mlp.cuh"
 #include "lbm_step.cuh"
 #include "lbmbin.hpp"
 #include "postprocess.hpp"
@@ -339,6 +340,11 @@ dim3 grid_1d(size_t N)
 template <typename MeanT>
 lbm_status launch_step(lbm_handle *h, bool monitored = false)
 {
+    if (h->closure) {
+        if (monitored)
+            return fail(LBM_ERR_STATE, "monitored steps are not available with the learned closure");
+        return lbm::closure_step(h);
+    }
     // the parameter block has the same layout for every storage type (the
     // output is a pointer); it is filled once here as the FP32 instance
     StepParams<MeanT> p{};
@@ -394,6 +400,8 @@ EncodeTiledFn encode_tiled() { return get_encode(); }
 
 lbm_status check_fault(const StepFault &f, const char *who)
 {
+    if (f.flags & ERR_MMA_TIMEOUT)
+        return fail(LBM_ERR_TIMEOUT, "the closure network timed out waiting for a tensor-core MMA");
     if (!(f.flags & ERR_TMA_TIMEOUT))
         return LBM_OK;
     std::string msg = std::string(who) + " timed out waiting for a TMA copy";
@@ -416,7 +424,7 @@ void destroy_handle(lbm_handle *h)
         cudaStreamSynchronize(h->stream);
     for (void *p : {h->m[0], h->m[1], static_cast<void *>(h->S), static_cast<void *>(h->k), h->SMean, h->kMean,
                     h->momentsMean, static_cast<void *>(h->err), static_cast<void *>(h->red),
-                    static_cast<void *>(h->mon), h->scratch})
+                    static_cast<void *>(h->mon), h->scratch, static_cast<void *>(h->dtau), h->mlp})
         if (p)
             cudaFree(p);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -1038,6 +1046,15 @@ lbm_status apply_variant(lbm_handle *h, int tx, int ty, int stages, int npb, int
 
 }  // namespace
 
+}  // extern "C"
+namespace lbm {
+lbm_status retile(lbm_handle *h, int tx, int ty, int stages, int npb, int zc)
+{
+    return apply_variant(h, tx, ty, stages, npb, zc);
+}
+}  // namespace lbm
+extern "C" {
+
 lbm_status lbm_autotune(lbm_handle *h, int32_t trial_steps, lbm_tuning *out)
 {
     if (!h)
@@ -1101,6 +1118,8 @@ lbm_status lbm_autotune(lbm_handle *h, int32_t trial_steps, lbm_tuning *out)
     for (const Variant &v : kVariants) {
         if (v.Q != h->Q || v.storage != h->storage || v.tx > h->cfg.nx || v.ty > h->cfg.ny)
             continue;
+        if (h->closure && (v.stages != 2 || v.npb != 1))
+            continue;  // shapes that have a closure kernel
         // z-chunks below 8 only for meshes too small to fill the GPU at 8
         // (such a chunk re-reads two planes for every 2-4 it updates)
         const int64_t tiles = ((h->cfg.nx + v.tx - 1) / v.tx) * ((h->cfg.ny + v.ty - 1) / v.ty);

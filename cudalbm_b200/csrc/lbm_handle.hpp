@@ -42,6 +42,10 @@ struct lbm_handle {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool timed = false;
     lbm::MonitorSlot *mon = nullptr;  // one slot, reused by every monitored step
+    // learned closure (lbm_closure.cu)
+    bool closure = false;
+    float *dtau = nullptr;             // [N] relaxation-time correction of the current step
+    void *mlp = nullptr;               // lbm::MlpDevice
 };
 
 namespace lbm {
@@ -60,6 +64,12 @@ void destroy_handle(lbm_handle *h);
 
 // LBM_OK, or the status and message for a device-side error record.
 lbm_status check_fault(const StepFault &f, const char *who);
+
+// Switch a handle to another compiled kernel shape (same results).
+lbm_status retile(lbm_handle *h, int tx, int ty, int stages, int npb, int zc);
+
+// One time step with the learned closure (lbm_closure.cu).
+lbm_status closure_step(lbm_handle *h);
 
 }  // namespace lbm
 

@@ -193,6 +193,7 @@ struct StepParams {
     FOPtrs<MeanT> fo;
     StepFault *fault;
     uint64_t timeout_ns;
+    const float *dtau;  // per-node relaxation-time correction (closure kernels only)
 };
 
 template <int TX, int TY, typename ST = float>
@@ -309,7 +310,7 @@ static __device__ __noinline__ void record_fault(StepFault *f, unsigned flag, in
 // keep cycling from one item to the next; the mbarriers are initialised once
 // per CTA.  Returns false, uniformly across the CTA, when a TMA wait timed
 // out (the error flag is then set).
-template <int Q, int TX, int TY, int NSTAGE, bool FO, typename MeanT, bool MON, int NPB, typename ST>
+template <int Q, int TX, int TY, int NSTAGE, bool FO, typename MeanT, bool MON, int NPB, typename ST, bool CL = false>
 __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepParams<MeanT, ST> &p, int bx, int by,
                                             int bz, unsigned g0, const CtaSmem<ST> &sh, int *s_abort, MonAcc &acc,
                                             int item = -1, int mesh = -1)
@@ -358,6 +359,11 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
         const bool upd = (i >= 2) && own;
         const size_t iu = size_t(zu) * plane + size_t(y) * p.nx + x;
         MeanT sm_old[6], km_old = MeanT(0);
+        float dtau = 0.0f;
+        if constexpr (CL) {
+            if (upd)
+                dtau = p.dtau[iu];
+        }
         if constexpr (FO) {
             if (upd) {
                 if (p.fo.SMean) {
@@ -434,7 +440,19 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
             if (own) {
                 const unsigned type = node_type(x, y, zu, p.nx, p.ny, p.nz);
                 float m[10];
-                node_update<Q>(f, type, p.rx, m);
+                if constexpr (CL) {
+                    // interior nodes relax with tau0 + dtau; omega as the host
+                    // derives it from tau, so dtau = 0 gives the plain bits
+                    Relax r = p.rx;
+                    if (!type) {
+                        r.omega = __fdiv_rn(1.0f, __fadd_rn(p.rx.tau, dtau));
+                        r.t_omega = __fsub_rn(1.0f, r.omega);
+                        r.omega_d2 = __fmul_rn(r.omega, 0.5f);
+                    }
+                    node_update<Q>(f, type, r, m);
+                } else {
+                    node_update<Q>(f, type, p.rx, m);
+                }
                 ST *o = p.out + iu;
                 o[0] = Storage<ST>::store(m[0] - 1.0f, 0);
 #pragma unroll
@@ -571,6 +589,26 @@ __global__ void __launch_bounds__(TX *TY, MINB)
                                                             &s_abort, acc);
     if constexpr (MON)
         monitor_flush<TX * TY>(acc, p.mon, lin);
+    if (s_abort && lin == 0)
+        drain_after_abort<NSTAGE>(sh.bars);
+}
+
+// One step with the learned closure: as step_kernel (no function objects,
+// FP32 storage), each interior node relaxing with tau0 + p.dtau[node].
+template <int Q, int TX, int TY, int NSTAGE, int NPB, int MINB>
+__global__ void __launch_bounds__(TX *TY, MINB)
+    closure_kernel(const __grid_constant__ CUtensorMap tmap_in, const StepParams<float, float> p)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ int s_abort;
+    const CtaSmem<float> sh = cta_smem<Q, TX, TY, NSTAGE, NPB, float>(smem);
+    const int lin = threadIdx.y * TX + threadIdx.x;
+    init_barriers<NSTAGE>(sh.bars, lin == 0);
+    s_abort = 0;
+    cta_sync();
+    MonAcc acc;
+    march_chunk<Q, TX, TY, NSTAGE, false, float, false, NPB, float, true>(&tmap_in, p, blockIdx.x, blockIdx.y,
+                                                                          blockIdx.z, 0u, sh, &s_abort, acc);
     if (s_abort && lin == 0)
         drain_after_abort<NSTAGE>(sh.bars);
 }

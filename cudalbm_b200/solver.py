@@ -125,6 +125,25 @@ class Cavity:
     def step(self, n: int = 1) -> None:
         _lib.check(_lib.lib().lbm_step(self._h, int(n)))
 
+    def perturb_velocity(self, amplitude: float, seed: int) -> None:
+        """Add U(-amplitude, amplitude) to u, v, w of every interior node."""
+        _lib.check(_lib.lib().lbm_perturb_velocity(self._h, float(amplitude), int(seed)))
+
+    def filter_from(self, fine: "Cavity") -> None:
+        """This (coarse) state := 2:1 box filter of `fine`'s current state."""
+        _lib.check(_lib.lib().lbm_filter_2to1(fine._h, self._h))
+
+    def set_closure(self, net) -> None:
+        """Relax every interior node with tau0 + dtau from the network `net`
+        (an _lib.MLP) in every following step; None restores the plain method."""
+        _lib.check(_lib.lib().lbm_closure_set(self._h, ctypes.byref(net) if net is not None else None))
+
+    def closure_dtau(self) -> np.ndarray:
+        nz, ny, nx = self.shape
+        out = np.empty((nz, ny, nx), np.float32)
+        _lib.check(_lib.lib().lbm_closure_dtau(self._h, out.ctypes.data, out.size))
+        return out
+
     def cut_plane(self, axis: int, position: float, field_set: str = "moments") -> np.ndarray:
         """Plane normal to `axis` (0 x, 1 y, 2 z) at `position` in [0, 1]
         between the first and last node plane, linearly interpolated on the

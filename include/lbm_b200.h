@@ -267,6 +267,87 @@ lbm_status lbm_batch_get_info(lbm_batch *b, lbm_batch_info *info);
  * compiled kernel has that shape. */
 lbm_status lbm_batch_configure(lbm_batch *b, const lbm_batch_tuning *shape);
 
+/* ------------------------------------------------------ learned closure
+ * A per-node network predicts a correction dtau to the relaxation time of
+ * an under-resolved run; no counterpart in the reference.  Network: 16
+ * features -> 32 -> 32 -> 1 with exact GELU.  Features of a node from its
+ * stored moments m (rho-1, 3u, 3v, 3w, 4.5 m_aa, 9 m_ab): the 10 moments and
+ * 3 (u_a u_b - m_ab) / (2 scale tau0) for ab = xx, xy, xz, yy, yz, zz, each
+ * standardised as (f - in_mean) * in_scale.  dtau = clamp(out_scale * y,
+ * dtau_lo, dtau_hi); nodes with any feature outside [in_lo, in_hi] (the range
+ * seen in training) and boundary nodes keep the plain collision. */
+typedef struct lbm_mlp {
+    float w1[32 * 16], b1[32];      /* layer 1, [out][in] */
+    float w2[32 * 32], b2[32];      /* layer 2, [out][in] */
+    float w3[32], b3;               /* output */
+    float in_mean[16], in_scale[16];
+    float in_lo[16], in_hi[16];
+    float out_scale, dtau_lo, dtau_hi;
+} lbm_mlp;
+
+typedef struct lbm_trainer lbm_trainer;
+
+typedef struct lbm_train_options {
+    int32_t steps;                  /* Adam steps */
+    int32_t batch;                  /* samples per step, drawn at random */
+    float lr;                       /* Adam learning rate */
+    float dtau_lo, dtau_hi;         /* targets are clipped to this range (also the inference clip) */
+    uint64_t seed;                  /* initial weights and batches */
+} lbm_train_options;
+
+typedef struct lbm_train_report {
+    uint64_t samples, steps;
+    double loss_first, loss_last;   /* mean squared error on standardised targets, first and last tenth */
+    double target_rms;              /* out_scale */
+} lbm_train_report;
+
+/* Add U(-amplitude, amplitude) to the velocity (lattice units) of every
+ * interior node of the current state, from a counter-based hash of `seed`. */
+lbm_status lbm_perturb_velocity(lbm_handle *h, float amplitude, uint64_t seed);
+
+/* coarse state := 2:1 box filter of the fine state (mean of the 8 fine
+ * nodes of every coarse node, all 10 stored moments; fine = 2 x coarse). */
+lbm_status lbm_filter_2to1(lbm_handle *fine, lbm_handle *coarse);
+
+/* Sample store for training, capacity in samples (16 features + 1 target). */
+lbm_status lbm_trainer_create(int32_t device, uint64_t capacity, lbm_trainer **out);
+lbm_status lbm_trainer_destroy(lbm_trainer *t);
+
+/* Training pairs from one coarse step: `coarse` holds F(t) (a filtered fine
+ * state) and is advanced one plain step by this call; `fine_next` is the
+ * fine run two fine steps later.  For every `stride`-th interior node: the
+ * features of F(t) and the dtau for which its collision gives the filtered
+ * fine state instead (first order).  *total = samples stored so far. */
+lbm_status lbm_trainer_add(lbm_trainer *t, lbm_handle *coarse, lbm_handle *fine_next, uint32_t stride,
+                           uint64_t *total);
+
+/* Copy stored samples [first, first+count) to the host (features [n][16],
+ * targets [n]; either may be NULL); *total = samples stored. */
+lbm_status lbm_trainer_samples(lbm_trainer *t, uint64_t first, uint64_t count, float *features, float *targets,
+                               uint64_t *total);
+
+/* Train a network on the stored samples with the GPU's forward/backward
+ * kernels and Adam; fills *net (weights, normalisation, ranges, clip). */
+lbm_status lbm_trainer_fit(lbm_trainer *t, const lbm_train_options *opt, lbm_mlp *net, lbm_train_report *rep);
+
+/* Gradient of the mean squared error over samples [first, first+count) for
+ * *net, from the training kernels (weights and biases of *grad filled, the
+ * rest zero); *loss = the error. */
+lbm_status lbm_trainer_gradient(lbm_trainer *t, const lbm_mlp *net, uint64_t first, uint64_t count, lbm_mlp *grad,
+                                double *loss);
+
+/* Raw network output y for host features [n][16]: tensor cores (FP16
+ * weights and activations, FP32 accumulation) or FP32 CUDA cores. */
+lbm_status lbm_mlp_infer(int32_t device, const lbm_mlp *net, const float *features, uint64_t n, float *y,
+                         int32_t tensor_cores);
+
+/* Use the network in every following lbm_step of this handle (NULL: back to
+ * the plain collision).  FP32 storage, no function objects. */
+lbm_status lbm_closure_set(lbm_handle *h, const lbm_mlp *net);
+
+/* The dtau field of the last closure step ([z][y][x], count = nodes). */
+lbm_status lbm_closure_dtau(lbm_handle *h, float *host, size_t count);
+
 /* Page-locked host memory for fast transfers (cudaMallocHost); free with
  * lbm_host_free.  Replaces: the reference's pinned host::array variant
  * (src/array/hostArray.cuh:66-140). */
