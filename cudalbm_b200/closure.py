@@ -45,9 +45,10 @@ class Trainer:
     def __exit__(self, *exc):
         self.close()
 
-    def add(self, coarse, fine_next, stride: int = 1) -> int:
+    def add(self, coarse, fine_next, stride: int = 1, min_neq: float = 0.0) -> int:
         total = ctypes.c_uint64()
-        _lib.check(_lib.lib().lbm_trainer_add(self._t, coarse._h, fine_next._h, int(stride), ctypes.byref(total)))
+        _lib.check(_lib.lib().lbm_trainer_add(self._t, coarse._h, fine_next._h, int(stride), float(min_neq),
+                                              ctypes.byref(total)))
         return total.value
 
     def __len__(self) -> int:

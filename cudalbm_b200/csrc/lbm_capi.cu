@@ -424,9 +424,10 @@ void destroy_handle(lbm_handle *h)
         cudaStreamSynchronize(h->stream);
     for (void *p : {h->m[0], h->m[1], static_cast<void *>(h->S), static_cast<void *>(h->k), h->SMean, h->kMean,
                     h->momentsMean, static_cast<void *>(h->err), static_cast<void *>(h->red),
-                    static_cast<void *>(h->mon), h->scratch, static_cast<void *>(h->dtau), h->mlp})
+                    static_cast<void *>(h->mon), h->scratch, static_cast<void *>(h->dtau)})
         if (p)
             cudaFree(p);
+    delete h->mlp;
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->stream && h->own_stream)

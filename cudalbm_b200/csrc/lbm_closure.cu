@@ -4,7 +4,8 @@
 // A per-node MLP predicts a correction dtau to the relaxation time of an
 // under-resolved run.  Pieces:
 //   * training data: a fine run (perturbed initial velocities) is box-filtered
-//     2:1 onto the coarse grid at coarse times t and t+1 (two fine steps);
+//     2:1 onto the coarse grid at coarse times t and t+1 (two fine steps),
+//     with its non-equilibrium stresses rescaled to the coarse lattice;
 //     the coarse solver advances the filtered state F(t) one plain step to C;
 //     the target at each interior node is the dtau for which the node's
 //     collision would have produced F(t+1) instead of C, to first order:
@@ -70,75 +71,162 @@ __global__ void perturb_kernel(float *m, int nx, int ny, int nz, float amp3, uin
     }
 }
 
-// coarse node (X, Y, Z) = mean of fine nodes (2X + a, 2Y + b, 2Z + c), every field
-__global__ void filter_kernel(float *coarse, const float *fine, int nx, int ny, int nz)
+// Coarse node (X, Y, Z) from fine nodes (2X + a, 2Y + b, 2Z + c): the mean of
+// rho - 1 and 3u, and for the second-order moments the mean of their
+// equilibrium part (u_a u_b in stored units, which keeps the subgrid part
+// mean(u_a u_b) - mean(u_a) mean(u_b)) plus kappa times the mean of their
+// non-equilibrium part, which the coarse lattice carries kappa times larger
+// (grid-refinement rescaling, see lbm_filter_2to1).
+__global__ void filter_kernel(float *coarse, const float *fine, int nx, int ny, int nz, float kappa)
 {
     const size_t Nc = size_t(nx) * ny * nz, Nf = Nc * 8;
     const int fx = 2 * nx, fy = 2 * ny;
-    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < Nc * 10; i += size_t(gridDim.x) * blockDim.x) {
-        const size_t k = i / Nc, j = i % Nc;
+    for (size_t j = blockIdx.x * size_t(blockDim.x) + threadIdx.x; j < Nc; j += size_t(gridDim.x) * blockDim.x) {
         const int x = int(j % nx), y = int((j / nx) % ny), z = int(j / (size_t(nx) * ny));
-        const float *f = fine + k * Nf;
-        float s = 0.0f;
+        float sum[10] = {}, eq[6] = {};
         for (int c = 0; c < 2; c++)
             for (int b = 0; b < 2; b++)
-                for (int a = 0; a < 2; a++)
-                    s += f[size_t(2 * x + a) + size_t(fx) * (size_t(2 * y + b) + size_t(fy) * size_t(2 * z + c))];
-        coarse[k * Nc + j] = s * 0.125f;
+                for (int a = 0; a < 2; a++) {
+                    const size_t i = size_t(2 * x + a) + size_t(fx) * (size_t(2 * y + b) + size_t(fy) * size_t(2 * z + c));
+                    float m[10];
+                    for (int k = 0; k < 10; k++)
+                        m[k] = fine[size_t(k) * Nf + i];
+                    for (int k = 0; k < 10; k++)
+                        sum[k] += m[k];
+                    eq[0] += 0.5f * m[1] * m[1];
+                    eq[1] += m[1] * m[2];
+                    eq[2] += m[1] * m[3];
+                    eq[3] += 0.5f * m[2] * m[2];
+                    eq[4] += m[2] * m[3];
+                    eq[5] += 0.5f * m[3] * m[3];
+                }
+        for (int k = 0; k < 4; k++)
+            coarse[size_t(k) * Nc + j] = sum[k] * 0.125f;
+        for (int k = 0; k < 6; k++)
+            coarse[size_t(4 + k) * Nc + j] = (eq[k] + kappa * (sum[4 + k] - eq[k])) * 0.125f;
     }
 }
 
-// One sample per selected interior node: features of F(t), target dtau.
-__global__ void target_kernel(const float *f0, const float *f1, const float *c, int nx, int ny, int nz,
-                              unsigned stride, float omega, float tau0, float r_ii, float r_ij, float *feat,
-                              float *targ, unsigned long long *count, unsigned long long cap)
+// kappa = 2 (tau_c / tau_f) (1 - omega_c) / (1 - omega_f): the ratio of the
+// stored (post-collision) non-equilibrium moments on the two lattices for the
+// same flow.  Pre-collision they scale with tau * S, S per lattice step twice
+// as large on the coarse lattice (dt_c = 2 dt_f at equal lattice velocity);
+// the collision multiplies them by (1 - omega).
+float refinement_kappa(const lbm_handle *fine, const lbm_handle *coarse)
 {
-    const size_t N = size_t(nx) * ny * nz;
-    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x) {
-        if (i % stride)
-            continue;
-        const int x = int(i % nx), y = int((i / nx) % ny), z = int(i / (size_t(nx) * ny));
-        if (lbm::node_type(x, y, z, nx, ny, nz))
-            continue;
-        float cm[10], r[6];
-        for (int k = 0; k < 10; k++)
-            cm[k] = c[size_t(k) * N + i];
-        const float u = cm[1], v = cm[2], w = cm[3];
-        const float eq[6] = {0.5f * u * u, u * v, u * w, 0.5f * v * v, v * w, 0.5f * w * w};
-        double num = 0.0, den = 0.0;
-        for (int k = 0; k < 6; k++) {
-            const double neq = double(cm[4 + k]) - double(eq[k]);
-            r[k] = f1[size_t(4 + k) * N + i] - cm[4 + k];
-            num += double(r[k]) * neq;
-            den += neq * neq;
+    return 2.0f * (coarse->tau / fine->tau) * (1.0f - coarse->omega) / (1.0f - fine->omega);
+}
+
+// Sample selection and target of node i (see the file header); false if the
+// node gives no sample (boundary, off-stride, too little non-equilibrium
+// stress for a stable ratio, or an unusable relaxation rate).
+struct TargetArgs {
+    const float *f0, *f1, *c;
+    int nx, ny, nz;
+    unsigned stride;
+    float omega, tau0, r_ii, r_ij;
+    double min_den;
+};
+__device__ bool node_target(const TargetArgs &a, size_t i, float &dtau)
+{
+    const size_t N = size_t(a.nx) * a.ny * a.nz;
+    if (i >= N || i % a.stride)
+        return false;
+    const int x = int(i % a.nx), y = int((i / a.nx) % a.ny), z = int(i / (size_t(a.nx) * a.ny));
+    if (lbm::node_type(x, y, z, a.nx, a.ny, a.nz))
+        return false;
+    float cm[10];
+    for (int k = 0; k < 10; k++)
+        cm[k] = a.c[size_t(k) * N + i];
+    const float u = cm[1], v = cm[2], w = cm[3];
+    const float eq[6] = {0.5f * u * u, u * v, u * w, 0.5f * v * v, v * w, 0.5f * w * w};
+    double num = 0.0, den = 0.0;
+    for (int k = 0; k < 6; k++) {
+        const double neq = double(cm[4 + k]) - double(eq[k]);
+        const double r = double(a.f1[size_t(4 + k) * N + i] - cm[4 + k]);
+        num += r * neq;
+        den += neq * neq;
+    }
+    if (!(den > a.min_den))
+        return false;
+    const double w_new = double(a.omega) - double(1.0f - a.omega) * num / den;
+    if (!(w_new > 0.0) || !(w_new < 2.0))
+        return false;
+    dtau = float(1.0 / w_new - double(a.tau0));
+    return isfinite(dtau);
+}
+
+// Samples are stored in node order, whatever the scheduling: CTA b owns the
+// nodes [b * kChunk, (b + 1) * kChunk); pass 1 counts its samples, the host
+// turns the counts into offsets, pass 2 writes them with in-CTA ranks from
+// warp ballots.
+constexpr int kSampleCta = 256;
+constexpr size_t kChunk = 8 * kSampleCta;
+
+__global__ void __launch_bounds__(kSampleCta) count_samples_kernel(TargetArgs a, unsigned *counts)
+{
+    const size_t base = size_t(blockIdx.x) * kChunk;
+    unsigned n = 0;
+    for (size_t r = 0; r < kChunk; r += kSampleCta) {
+        float d;
+        n += node_target(a, base + r + threadIdx.x, d);
+    }
+    for (int o = 16; o > 0; o >>= 1)
+        n += __shfl_down_sync(0xffffffffu, n, o);
+    __shared__ unsigned warp_n[kSampleCta / 32];
+    if ((threadIdx.x & 31) == 0)
+        warp_n[threadIdx.x >> 5] = n;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned t = 0;
+        for (int w = 0; w < kSampleCta / 32; w++)
+            t += warp_n[w];
+        counts[blockIdx.x] = t;
+    }
+}
+
+__global__ void __launch_bounds__(kSampleCta) write_samples_kernel(TargetArgs a, const unsigned long long *offsets,
+                                                                   float *feat, float *targ, unsigned long long cap)
+{
+    __shared__ unsigned warp_n[kSampleCta / 32];
+    const size_t N = size_t(a.nx) * a.ny * a.nz;
+    const size_t base = size_t(blockIdx.x) * kChunk;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long next = offsets[blockIdx.x];
+    for (size_t r = 0; r < kChunk; r += kSampleCta) {
+        const size_t i = base + r + threadIdx.x;
+        float dtau = 0.0f;
+        const bool ok = node_target(a, i, dtau);
+        const unsigned ballot = __ballot_sync(0xffffffffu, ok);
+        if (lane == 0)
+            warp_n[warp] = __popc(ballot);
+        __syncthreads();
+        unsigned before = 0, total = 0;
+        for (int w = 0; w < kSampleCta / 32; w++) {
+            before += w < warp ? warp_n[w] : 0u;
+            total += warp_n[w];
         }
-        if (!(den > 1e-24))
-            continue;
-        const double w_new = double(omega) - double(1.0f - omega) * num / den;
-        if (!(w_new > 0.0) || !(w_new < 2.0))
-            continue;
-        const float dtau = float(1.0 / w_new - double(tau0));
-        if (!isfinite(dtau))
-            continue;
-        const unsigned long long slot = atomicAdd(count, 1ull);
-        if (slot >= cap)
-            continue;
-        float m[10], fv[kMlpIn];
-        for (int k = 0; k < 10; k++)
-            m[k] = f0[size_t(k) * N + i];
-        lbm::node_features(m, r_ii, r_ij, fv);
-        for (int k = 0; k < kMlpIn; k++)
-            feat[slot * kMlpIn + k] = fv[k];
-        targ[slot] = dtau;
+        const unsigned long long slot = next + before + __popc(ballot & ((1u << lane) - 1u));
+        if (ok && slot < cap) {
+            float m[10], fv[kMlpIn];
+            for (int k = 0; k < 10; k++)
+                m[k] = a.f0[size_t(k) * N + i];
+            lbm::node_features(m, a.r_ii, a.r_ij, fv);
+            for (int k = 0; k < kMlpIn; k++)
+                feat[slot * kMlpIn + k] = fv[k];
+            targ[slot] = dtau;
+        }
+        next += total;
+        __syncthreads();
     }
 }
 
 // ----------------------------------------------------- training kernels
+// d gelu / dz of the tanh form
 __device__ __forceinline__ float gelu_grad(float z)
 {
-    const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
-    const float pdf = 0.39894228040143268f * expf(-0.5f * z * z);
-    return cdf + z * pdf;
+    const float t = tanhf(lbm::kGeluA * fmaf(lbm::kGeluB * z * z, z, z));
+    return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * lbm::kGeluA * fmaf(3.0f * lbm::kGeluB, z * z, 1.0f);
 }
 
 // Mean squared error gradient over a batch.  Sample s of the batch is
@@ -157,7 +245,7 @@ struct TrainSmem {
 
 __global__ void __launch_bounds__(kTrainCta) grad_kernel(const float *feat, const float *targ, uint64_t n,
                                                          uint64_t first, uint64_t batch, uint64_t seed, int random,
-                                                         const MlpParams *params, float *grad, double *loss)
+                                                         const MlpParams *params, float *partial, double *loss_partial)
 {
     extern __shared__ __align__(16) unsigned char raw[];
     TrainSmem &S = *reinterpret_cast<TrainSmem *>(raw);
@@ -198,12 +286,20 @@ __global__ void __launch_bounds__(kTrainCta) grad_kernel(const float *feat, cons
     for (int k = 0; k < kMlpIn; k++)
         S.xs[t][k] = xs[k];
     S.dy[t] = dy;
-    // block sum of the squared errors
+    // CTA sum of the squared errors, in a fixed order
+    double e2d = double(e2);
     for (int o = 16; o > 0; o >>= 1)
-        e2 += __shfl_down_sync(0xffffffffu, e2, o);
-    if ((t & 31) == 0 && e2 != 0.0f)
-        atomicAdd(loss, double(e2));
+        e2d += __shfl_down_sync(0xffffffffu, e2d, o);
+    __shared__ double warp_e2[kTrainCta / 32];
+    if ((t & 31) == 0)
+        warp_e2[t >> 5] = e2d;
     __syncthreads();
+    if (t == 0) {
+        double sum = 0.0;
+        for (int w = 0; w < kTrainCta / 32; w++)
+            sum += warp_e2[w];
+        loss_partial[blockIdx.x] = sum;
+    }
     // phase 2: parameter p (the lbm_mlp weight order w1, b1, w2, b2, w3, b3)
     for (int p = t; p < kMlpWeights; p += kTrainCta) {
         float acc = 0.0f;
@@ -229,7 +325,26 @@ __global__ void __launch_bounds__(kTrainCta) grad_kernel(const float *feat, cons
             for (int r = 0; r < kTrainCta; r++)
                 acc += S.dy[r];
         }
-        atomicAdd(&grad[p], acc);
+        partial[size_t(blockIdx.x) * kMlpWeights + p] = acc;
+    }
+}
+
+// Sum of the CTAs' partial gradients (and losses), in CTA order.
+__global__ void reduce_partials_kernel(const float *partial, const double *loss_partial, int ctas, float *grad,
+                                       double *loss)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < kMlpWeights) {
+        float s = 0.0f;
+        for (int b = 0; b < ctas; b++)
+            s += partial[size_t(b) * kMlpWeights + p];
+        grad[p] = s;
+    }
+    if (p == 0) {
+        double l = 0.0;
+        for (int b = 0; b < ctas; b++)
+            l += loss_partial[b];
+        *loss = l;
     }
 }
 
@@ -274,8 +389,9 @@ MlpDevice device_copy(const MlpParams &p, float tau0)
     std::memcpy(d.b2, p.b2, sizeof(d.b2));
     std::memcpy(d.w3, p.w3, sizeof(d.w3));
     d.b3 = p.b3;
-    std::memcpy(d.in_mean, p.in_mean, sizeof(d.in_mean));
     std::memcpy(d.in_scale, p.in_scale, sizeof(d.in_scale));
+    for (int k = 0; k < kMlpIn; k++)
+        d.in_shift[k] = -p.in_mean[k] * p.in_scale[k];
     std::memcpy(d.in_lo, p.in_lo, sizeof(d.in_lo));
     std::memcpy(d.in_hi, p.in_hi, sizeof(d.in_hi));
     d.out_scale = p.out_scale;
@@ -286,7 +402,7 @@ MlpDevice device_copy(const MlpParams &p, float tau0)
     return d;
 }
 
-lbm_status launch_infer(const float *src, size_t N, const MlpDevice *net, float *out, unsigned *err, bool from_moments,
+lbm_status launch_infer(const float *src, size_t N, const MlpDevice &net, float *out, unsigned *err, bool from_moments,
                         bool raw_y, cudaStream_t stream, int device)
 {
     void *fn = from_moments ? (raw_y ? (void *)&lbm::mlp_infer_kernel<true, true> : (void *)&lbm::mlp_infer_kernel<true, false>)
@@ -296,9 +412,11 @@ lbm_status launch_infer(const float *src, size_t N, const MlpDevice *net, float 
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     const size_t tiles = (N + 127) / 128;
-    const unsigned grid = unsigned(std::min<size_t>(tiles, size_t(sms) * 4));
+    // 8 CTAs per SM: the register limit at 64 per thread (8 x 32 tensor-memory columns fit)
+    const unsigned grid = unsigned(std::min<size_t>(tiles, size_t(sms) * 8));
     uint64_t timeout = 2000000000ull;
-    void *args[] = {&src, &N, &net, &out, &err, &timeout};
+    MlpDevice net_arg = net;
+    void *args[] = {&src, &N, &net_arg, &out, &err, &timeout};
     LBM_CUDA_RETURN(cudaLaunchKernel(fn, dim3(grid), dim3(128), args, lbm::MlpSmem::LAUNCH_BYTES, stream));
     return LBM_OK;
 }
@@ -328,8 +446,11 @@ struct lbm_trainer {
     int device = 0;
     uint64_t cap = 0;
     float *feat = nullptr, *targ = nullptr;
-    unsigned long long *count = nullptr;
+    uint64_t n = 0;            // samples stored (at most cap)
     float *scratch = nullptr;  // F(t) copy and filtered F(t+1) of the coarse grid
+    unsigned *counts = nullptr;            // per-CTA sample counts of one lbm_trainer_add
+    unsigned long long *offsets = nullptr;  // and their offsets
+    size_t count_slots = 0;
     size_t scratch_floats = 0;
     cudaStream_t stream = nullptr;
 };
@@ -340,10 +461,13 @@ namespace lbm {
 // the tensor cores, then the closure step kernel.
 lbm_status closure_step(lbm_handle *h)
 {
-    lbm_status s = launch_infer(static_cast<const float *>(h->m[h->cur]), h->N, static_cast<const MlpDevice *>(h->mlp),
-                                h->dtau, &h->err->flags, true, false, h->stream, h->cfg.device);
-    if (s != LBM_OK)
-        return s;
+    if (h->closure_steps++ % uint64_t(h->closure_every) == 0) {
+        lbm_status s = launch_infer(static_cast<const float *>(h->m[h->cur]), h->N, *h->mlp, h->dtau,
+                                    &h->err->flags, true, false, h->stream, h->cfg.device);
+        if (s != LBM_OK)
+            return s;
+        h->launches += 1;
+    }
     void *fn = nullptr;
     size_t smem = 0;
     if (!pick_closure(h->Q, h->launcher.tx, h->launcher.ty, h->launcher.stages, h->launcher.pop_buffers, fn, smem))
@@ -367,7 +491,7 @@ lbm_status closure_step(lbm_handle *h)
     LBM_CUDA_RETURN(cudaLaunchKernel(fn, grid, block, args, smem, h->stream));
     h->cur = nxt;
     h->t += 1;
-    h->launches += 2;
+    h->launches += 1;
     return LBM_OK;
 }
 
@@ -400,9 +524,9 @@ lbm_status lbm_filter_2to1(lbm_handle *fine, lbm_handle *coarse)
         return fail(LBM_ERR_ARG, "lbm_filter_2to1: FP32 storage on one device");
     LBM_CUDA_RETURN(cudaSetDevice(fine->cfg.device));
     LBM_CUDA_RETURN(cudaStreamSynchronize(fine->stream));
-    filter_kernel<<<grid_for(coarse->N * 10), 256, 0, coarse->stream>>>(
+    filter_kernel<<<grid_for(coarse->N), 256, 0, coarse->stream>>>(
         static_cast<float *>(coarse->m[coarse->cur]), static_cast<const float *>(fine->m[fine->cur]),
-        int(coarse->cfg.nx), int(coarse->cfg.ny), int(coarse->cfg.nz));
+        int(coarse->cfg.nx), int(coarse->cfg.ny), int(coarse->cfg.nz), refinement_kappa(fine, coarse));
     LBM_CUDA_RETURN(cudaGetLastError());
     coarse->launches += 1;
     LBM_CUDA_RETURN(cudaStreamSynchronize(coarse->stream));
@@ -420,12 +544,10 @@ lbm_status lbm_trainer_create(int32_t device, uint64_t capacity, lbm_trainer **o
     t->cap = capacity;
     if (cudaMalloc(&t->feat, capacity * kMlpIn * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&t->targ, capacity * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&t->count, sizeof(unsigned long long)) != cudaSuccess ||
         cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking) != cudaSuccess) {
         lbm_trainer_destroy(t);
         return fail(LBM_ERR_NOMEM, "lbm_trainer_create: cannot allocate the sample buffers");
     }
-    cudaMemset(t->count, 0, sizeof(unsigned long long));
     *out = t;
     return LBM_OK;
 }
@@ -437,8 +559,8 @@ lbm_status lbm_trainer_destroy(lbm_trainer *t)
     cudaSetDevice(t->device);
     if (t->stream)
         cudaStreamSynchronize(t->stream);
-    for (void *p : {static_cast<void *>(t->feat), static_cast<void *>(t->targ), static_cast<void *>(t->count),
-                    static_cast<void *>(t->scratch)})
+    for (void *p : {static_cast<void *>(t->feat), static_cast<void *>(t->targ), static_cast<void *>(t->counts),
+                    static_cast<void *>(t->offsets), static_cast<void *>(t->scratch)})
         if (p)
             cudaFree(p);
     if (t->stream)
@@ -447,7 +569,8 @@ lbm_status lbm_trainer_destroy(lbm_trainer *t)
     return LBM_OK;
 }
 
-lbm_status lbm_trainer_add(lbm_trainer *t, lbm_handle *coarse, lbm_handle *fine_next, uint32_t stride, uint64_t *total)
+lbm_status lbm_trainer_add(lbm_trainer *t, lbm_handle *coarse, lbm_handle *fine_next, uint32_t stride, float min_neq,
+                           uint64_t *total)
 {
     if (!t || !coarse || !fine_next || stride == 0)
         return fail(LBM_ERR_ARG, "lbm_trainer_add: null argument or zero stride");
@@ -473,23 +596,58 @@ lbm_status lbm_trainer_add(lbm_trainer *t, lbm_handle *coarse, lbm_handle *fine_
     LBM_CUDA_RETURN(cudaStreamSynchronize(coarse->stream));
     LBM_CUDA_RETURN(cudaMemcpyAsync(f0, coarse->m[coarse->cur], 10 * N * sizeof(float), cudaMemcpyDeviceToDevice,
                                     coarse->stream));
-    filter_kernel<<<grid_for(N * 10), 256, 0, coarse->stream>>>(f1, static_cast<const float *>(fine_next->m[fine_next->cur]),
-                                                                int(coarse->cfg.nx), int(coarse->cfg.ny), int(coarse->cfg.nz));
+    filter_kernel<<<grid_for(N), 256, 0, coarse->stream>>>(f1, static_cast<const float *>(fine_next->m[fine_next->cur]),
+                                                           int(coarse->cfg.nx), int(coarse->cfg.ny), int(coarse->cfg.nz),
+                                                           refinement_kappa(fine_next, coarse));
     LBM_CUDA_RETURN(cudaGetLastError());
     lbm_status s = lbm_step(coarse, 1);
     if (s != LBM_OK)
         return s;
-    const float r_ii = 1.0f / (2.0f * 4.5f * coarse->tau), r_ij = 1.0f / (2.0f * 9.0f * coarse->tau);
-    target_kernel<<<grid_for(N), 256, 0, coarse->stream>>>(
-        f0, f1, static_cast<const float *>(coarse->m[coarse->cur]), int(coarse->cfg.nx), int(coarse->cfg.ny),
-        int(coarse->cfg.nz), stride, coarse->omega, coarse->tau, r_ii, r_ij, t->feat, t->targ, t->count, t->cap);
+    TargetArgs a;
+    a.f0 = f0;
+    a.f1 = f1;
+    a.c = static_cast<const float *>(coarse->m[coarse->cur]);
+    a.nx = int(coarse->cfg.nx);
+    a.ny = int(coarse->cfg.ny);
+    a.nz = int(coarse->cfg.nz);
+    a.stride = stride;
+    a.omega = coarse->omega;
+    a.tau0 = coarse->tau;
+    a.r_ii = 1.0f / (2.0f * 4.5f * coarse->tau);
+    a.r_ij = 1.0f / (2.0f * 9.0f * coarse->tau);
+    a.min_den = std::max(1e-24, 6.0 * double(min_neq) * double(min_neq));
+    const size_t ctas = (N + kChunk - 1) / kChunk;
+    if (t->count_slots < ctas) {
+        cudaFree(t->counts);
+        cudaFree(t->offsets);
+        t->counts = nullptr;
+        t->offsets = nullptr;
+        t->count_slots = 0;
+        LBM_CUDA_RETURN(cudaMalloc(&t->counts, ctas * sizeof(unsigned)));
+        LBM_CUDA_RETURN(cudaMalloc(&t->offsets, ctas * sizeof(unsigned long long)));
+        t->count_slots = ctas;
+    }
+    count_samples_kernel<<<unsigned(ctas), kSampleCta, 0, coarse->stream>>>(a, t->counts);
     LBM_CUDA_RETURN(cudaGetLastError());
-    coarse->launches += 2;
-    unsigned long long n = 0;
-    LBM_CUDA_RETURN(cudaMemcpyAsync(&n, t->count, sizeof(n), cudaMemcpyDeviceToHost, coarse->stream));
+    std::vector<unsigned> counts(ctas);
+    std::vector<unsigned long long> offsets(ctas);
+    LBM_CUDA_RETURN(cudaMemcpyAsync(counts.data(), t->counts, ctas * sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                    coarse->stream));
     LBM_CUDA_RETURN(cudaStreamSynchronize(coarse->stream));
+    unsigned long long run = t->n;
+    for (size_t b = 0; b < ctas; b++) {
+        offsets[b] = run;
+        run += counts[b];
+    }
+    LBM_CUDA_RETURN(cudaMemcpyAsync(t->offsets, offsets.data(), ctas * sizeof(unsigned long long),
+                                    cudaMemcpyHostToDevice, coarse->stream));
+    write_samples_kernel<<<unsigned(ctas), kSampleCta, 0, coarse->stream>>>(a, t->offsets, t->feat, t->targ, t->cap);
+    LBM_CUDA_RETURN(cudaGetLastError());
+    LBM_CUDA_RETURN(cudaStreamSynchronize(coarse->stream));
+    coarse->launches += 3;
+    t->n = std::min<uint64_t>(run, t->cap);
     if (total)
-        *total = std::min<uint64_t>(n, t->cap);
+        *total = t->n;
     return LBM_OK;
 }
 
@@ -499,9 +657,7 @@ lbm_status lbm_trainer_samples(lbm_trainer *t, uint64_t first, uint64_t count, f
     if (!t)
         return fail(LBM_ERR_ARG, "null trainer");
     LBM_CUDA_RETURN(cudaSetDevice(t->device));
-    unsigned long long n = 0;
-    LBM_CUDA_RETURN(cudaMemcpy(&n, t->count, sizeof(n), cudaMemcpyDeviceToHost));
-    n = std::min<unsigned long long>(n, t->cap);
+    const uint64_t n = t->n;
     if (total)
         *total = n;
     if (count == 0)
@@ -527,25 +683,29 @@ lbm_status lbm_trainer_gradient(lbm_trainer *t, const lbm_mlp *net, uint64_t fir
         return s;
     if (first + count > n)
         return fail(LBM_ERR_ARG, "lbm_trainer_gradient: range beyond the stored samples");
+    const unsigned ctas = unsigned((count + kTrainCta - 1) / kTrainCta);
     MlpParams *dp = nullptr;
-    float *dg = nullptr;
-    double *dl = nullptr;
+    float *dg = nullptr, *dpart = nullptr;
+    double *dl = nullptr, *dlpart = nullptr;
     auto release = [&]() {
         cudaFree(dp);
         cudaFree(dg);
         cudaFree(dl);
+        cudaFree(dpart);
+        cudaFree(dlpart);
     };
     if (cudaMalloc(&dp, sizeof(MlpParams)) != cudaSuccess || cudaMalloc(&dg, sizeof(MlpParams)) != cudaSuccess ||
-        cudaMalloc(&dl, sizeof(double)) != cudaSuccess) {
+        cudaMalloc(&dl, sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&dpart, size_t(ctas) * kMlpWeights * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&dlpart, ctas * sizeof(double)) != cudaSuccess) {
         release();
         return fail(LBM_ERR_NOMEM, "lbm_trainer_gradient: no device memory");
     }
     cudaMemcpy(dp, net, sizeof(MlpParams), cudaMemcpyHostToDevice);
-    cudaMemset(dg, 0, sizeof(MlpParams));
-    cudaMemset(dl, 0, sizeof(double));
     cudaFuncSetAttribute(grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(TrainSmem)));
-    grad_kernel<<<unsigned((count + kTrainCta - 1) / kTrainCta), kTrainCta, sizeof(TrainSmem), t->stream>>>(
-        t->feat, t->targ, n, first, count, 0, 0, dp, dg, dl);
+    grad_kernel<<<ctas, kTrainCta, sizeof(TrainSmem), t->stream>>>(t->feat, t->targ, n, first, count, 0, 0, dp,
+                                                                   dpart, dlpart);
+    reduce_partials_kernel<<<(kMlpWeights + 255) / 256, 256, 0, t->stream>>>(dpart, dlpart, int(ctas), dg, dl);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(t->stream);
@@ -619,19 +779,25 @@ lbm_status lbm_trainer_fit(lbm_trainer *t, const lbm_train_options *opt, lbm_mlp
     for (float &w : P.w3)
         w = uni(a3);
     LBM_CUDA_RETURN(cudaSetDevice(t->device));
+    const uint64_t B = uint64_t(opt->batch);
+    const unsigned blocks = unsigned((B + kTrainCta - 1) / kTrainCta);
     MlpParams *dp = nullptr;
-    float *dg = nullptr, *dm = nullptr, *dv = nullptr;
-    double *dl = nullptr;
+    float *dg = nullptr, *dm = nullptr, *dv = nullptr, *dpart = nullptr;
+    double *dl = nullptr, *dlpart = nullptr;
     auto release = [&]() {
         cudaFree(dp);
         cudaFree(dg);
         cudaFree(dm);
         cudaFree(dv);
         cudaFree(dl);
+        cudaFree(dpart);
+        cudaFree(dlpart);
     };
     if (cudaMalloc(&dp, sizeof(MlpParams)) != cudaSuccess || cudaMalloc(&dg, kMlpWeights * 4) != cudaSuccess ||
         cudaMalloc(&dm, kMlpWeights * 4) != cudaSuccess || cudaMalloc(&dv, kMlpWeights * 4) != cudaSuccess ||
-        cudaMalloc(&dl, sizeof(double)) != cudaSuccess) {
+        cudaMalloc(&dl, sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&dpart, size_t(blocks) * kMlpWeights * 4) != cudaSuccess ||
+        cudaMalloc(&dlpart, blocks * sizeof(double)) != cudaSuccess) {
         release();
         return fail(LBM_ERR_NOMEM, "lbm_trainer_fit: no device memory");
     }
@@ -639,17 +805,14 @@ lbm_status lbm_trainer_fit(lbm_trainer *t, const lbm_train_options *opt, lbm_mlp
     cudaMemset(dm, 0, kMlpWeights * 4);
     cudaMemset(dv, 0, kMlpWeights * 4);
     cudaFuncSetAttribute(grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(TrainSmem)));
-    const uint64_t B = uint64_t(opt->batch);
-    const unsigned blocks = unsigned((B + kTrainCta - 1) / kTrainCta);
     double first_loss = -1.0, last_loss = 0.0;
     const int window = std::max(1, std::min(opt->steps / 10, 100));
     double acc = 0.0;
     int acc_n = 0;
     for (int step = 0; step < opt->steps; step++) {
-        cudaMemsetAsync(dg, 0, kMlpWeights * 4, t->stream);
-        cudaMemsetAsync(dl, 0, sizeof(double), t->stream);
         grad_kernel<<<blocks, kTrainCta, sizeof(TrainSmem), t->stream>>>(
-            t->feat, t->targ, n, 0, B, splitmix64(opt->seed + 0x51ED27ull * uint64_t(step + 1)), 1, dp, dg, dl);
+            t->feat, t->targ, n, 0, B, splitmix64(opt->seed + 0x51ED27ull * uint64_t(step + 1)), 1, dp, dpart, dlpart);
+        reduce_partials_kernel<<<(kMlpWeights + 255) / 256, 256, 0, t->stream>>>(dpart, dlpart, int(blocks), dg, dl);
         const float c1 = 1.0f / (1.0f - std::pow(0.9f, float(step + 1)));
         const float c2 = 1.0f / (1.0f - std::pow(0.999f, float(step + 1)));
         adam_kernel<<<(kMlpWeights + 255) / 256, 256, 0, t->stream>>>(reinterpret_cast<float *>(dp), dg, dm, dv,
@@ -715,9 +878,7 @@ lbm_status lbm_mlp_infer(int32_t device, const lbm_mlp *net, const float *featur
     cudaMemset(derr, 0, 4);
     lbm_status s = LBM_OK;
     if (tensor_cores) {
-        const MlpDevice d = device_copy(P, 1.0f);
-        cudaMemcpy(dn, &d, sizeof(d), cudaMemcpyHostToDevice);
-        s = launch_infer(df, n, static_cast<const MlpDevice *>(dn), dy, derr, false, true, nullptr, device);
+        s = launch_infer(df, n, device_copy(P, 1.0f), dy, derr, false, true, nullptr, device);
     } else {
         cudaMemcpy(dn, &P, sizeof(P), cudaMemcpyHostToDevice);
         forward_kernel<<<grid_for(n), 256>>>(df, n, static_cast<const MlpParams *>(dn), dy);
@@ -765,16 +926,22 @@ lbm_status lbm_closure_set(lbm_handle *h, const lbm_mlp *net)
         h->device_bytes += h->N * sizeof(float);
         LBM_CUDA_RETURN(cudaMemsetAsync(h->dtau, 0, h->N * sizeof(float), h->stream));
     }
-    if (!h->mlp) {
-        LBM_CUDA_RETURN(cudaMalloc(&h->mlp, sizeof(MlpDevice)));
-        h->device_bytes += sizeof(MlpDevice);
-    }
+    if (!h->mlp)
+        h->mlp = new MlpDevice();
     MlpParams P;
     std::memcpy(&P, net, sizeof(P));
-    const MlpDevice d = device_copy(P, h->tau);
-    LBM_CUDA_RETURN(cudaStreamSynchronize(h->stream));
-    LBM_CUDA_RETURN(cudaMemcpy(h->mlp, &d, sizeof(d), cudaMemcpyHostToDevice));
+    *h->mlp = device_copy(P, h->tau);
     h->closure = true;
+    h->closure_steps = 0;
+    return LBM_OK;
+}
+
+lbm_status lbm_closure_refresh(lbm_handle *h, int32_t every)
+{
+    if (!h || every < 1)
+        return fail(LBM_ERR_ARG, "lbm_closure_refresh: null handle or interval below 1");
+    h->closure_every = every;
+    h->closure_steps = 0;
     return LBM_OK;
 }
 

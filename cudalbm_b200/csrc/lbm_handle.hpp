@@ -10,6 +10,7 @@
 
 #include "lbm_b200.h"
 #include "lbm_step.cuh"
+#include "lbm_mlp.cuh"
 #include "lbm_variants.cuh"
 
 struct lbm_batch;
@@ -45,7 +46,9 @@ struct lbm_handle {
     // learned closure (lbm_closure.cu)
     bool closure = false;
     float *dtau = nullptr;             // [N] relaxation-time correction of the current step
-    void *mlp = nullptr;               // lbm::MlpDevice
+    lbm::MlpDevice *mlp = nullptr;     // network for the closure (host copy, passed by value)
+    int closure_every = 1;             // recompute dtau every this many steps
+    uint64_t closure_steps = 0;        // closure steps taken since lbm_closure_set
 };
 
 namespace lbm {

@@ -1,7 +1,8 @@
 // lbm_mlp.cuh -- the learned closure's per-node network on sm_100a.
 //
-// Network (fixed shape): 16 features -> 32 -> 32 -> 1, exact GELU after both
-// hidden layers.  Features of a node, from its stored (post-collision)
+// Network (fixed shape): 16 features -> 32 -> 32 -> 1, GELU after both hidden
+// layers in its tanh form (Hendrycks & Gimpel 2016):
+//     gelu(x) = 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))).  Features of a node, from its stored (post-collision)
 // moments m: the 10 moments themselves and the six strain-rate components
 // 3 (u_a u_b - m_ab) / (2 scale tau0) (the strain-rate function object's
 // formula); each standardised as (f - mean) * scale.  Output y; the closure
@@ -17,8 +18,9 @@
 //     thread issues tcgen05.mma (kind::f16, FP32 accumulators in tensor
 //     memory) for 16 -> 32, every warp reads its 32 rows back with
 //     tcgen05.ld, applies bias + GELU, writes FP16 activations for 32 -> 32
-//     (two K = 16 MMAs), reads back, and finishes the 32 -> 1 layer on CUDA
-//     cores.  Weights are FP16 (converted once on the host into the operand
+//     (two K = 16 MMAs into the same 32 tensor-memory columns), reads back,
+//     and finishes the 32 -> 1 layer on CUDA cores; the next tile's node
+//     values are loaded meanwhile.  Weights are FP16 (converted once on the host into the operand
 //     layout), accumulation FP32.
 #pragma once
 
@@ -50,7 +52,7 @@ struct MlpDevice {
     __half w1[kMlpHidden * kMlpIn];
     __half w2[kMlpHidden * kMlpHidden];
     float b1[kMlpHidden], b2[kMlpHidden], w3[kMlpHidden], b3;
-    float in_mean[kMlpIn], in_scale[kMlpIn], in_lo[kMlpIn], in_hi[kMlpIn];
+    float in_scale[kMlpIn], in_shift[kMlpIn], in_lo[kMlpIn], in_hi[kMlpIn];  // x = f * scale + shift
     float out_scale, dtau_lo, dtau_hi;
     float r_ii, r_ij;  // 1 / (2 * 4.5 * tau0), 1 / (2 * 9 * tau0) for the strain-rate features
 };
@@ -64,9 +66,36 @@ __host__ __device__ constexpr int umma_index(int row, int k, int rows)
     return ((k >> 3) * (rows >> 3) + (row >> 3)) * 64 + (row & 7) * 8 + (k & 7);
 }
 
+constexpr float kGeluA = 0.79788456080286536f, kGeluB = 0.044715f;  // sqrt(2/pi), cubic coefficient
+
+// accurate tanh (training and the FP32 path)
 __device__ __forceinline__ float gelu(float x)
 {
-    return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f));
+    return 0.5f * x * (1.0f + tanhf(kGeluA * fmaf(kGeluB * x * x, x, x)));
+}
+// hardware tanh (tanh.approx.f32; its error is below the FP16 rounding of
+// the activations that follow) for the tensor-core path
+__device__ __forceinline__ float gelu_fast(float x)
+{
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(kGeluA * fmaf(kGeluB * x * x, x, x)));
+    return 0.5f * x * (1.0f + t);
+}
+
+// One row (one node) of an FP16 operand in umma_index layout: K values, stored
+// as K/8 16-byte vectors (consecutive rows are consecutive 16-byte slots of a
+// core matrix, so a warp's stores do not conflict).
+template <int K>
+__device__ __forceinline__ void store_row_f16(__half *base, int row, const float *v)
+{
+#pragma unroll
+    for (int c = 0; c < K / 8; c++) {
+        __align__(16) __half2 h[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            h[j] = __floats2half2_rn(v[8 * c + 2 * j], v[8 * c + 2 * j + 1]);
+        *reinterpret_cast<uint4 *>(base + umma_index(row, 8 * c, 128)) = *reinterpret_cast<const uint4 *>(h);
+    }
 }
 
 // The 16 raw features of a node from its 10 stored moments (rho - 1, 3u, ...).
@@ -222,9 +251,9 @@ struct MlpSmem {
     static constexpr int TMEM = BAR + 8;                      // allocated tensor-memory address
     static constexpr int FLAG = TMEM + 4;                     // abort flag
     static constexpr int BYTES = FLAG + 4;
-    // shared memory requested per CTA: at most 7 CTAs fit on an SM (227 KB),
-    // so their 7 x 64 tensor-memory columns never exceed the SM's 512
-    static constexpr int LAUNCH_BYTES = 29 * 1024;
+    // shared memory requested per CTA: with at most 14 CTAs on an SM (227 KB),
+    // their 14 x 32 tensor-memory columns never exceed the SM's 512
+    static constexpr int LAUNCH_BYTES = 16 * 1024;
     // leading (K-chunk) byte offsets of the operands; the stride between
     // 8-row groups is 128 B for all of them
     static constexpr uint32_t LBO_W = (kMlpHidden / 8) * 128, LBO_A = (128 / 8) * 128, SBO = 128;
@@ -232,12 +261,14 @@ struct MlpSmem {
 
 enum : unsigned { ERR_MMA_TIMEOUT = 2u };
 
-// Source of a node's 16 raw features: stored moments [10][N] (FROM_MOMENTS)
+// The network is a kernel parameter (constant bank: its uniform values feed
+// instructions directly).  Source of a node's 16 raw features: stored moments [10][N] (FROM_MOMENTS)
 // or a feature array [N][16].  Output dtau[N] (clamped, 0 where the inputs
 // leave the training range), or the raw network output y[N] (RAW_Y).
 template <bool FROM_MOMENTS, bool RAW_Y>
-__global__ void __launch_bounds__(128) mlp_infer_kernel(const float *src, size_t N, const MlpDevice *net,
-                                                        float *out, unsigned *err, uint64_t timeout_ns)
+__global__ void __launch_bounds__(128, 8) mlp_infer_kernel(const float *src, size_t N,
+                                                           const __grid_constant__ MlpDevice net, float *out,
+                                                           unsigned *err, uint64_t timeout_ns)
 {
     extern __shared__ __align__(1024) unsigned char sm[];
     __half *w1 = reinterpret_cast<__half *>(sm + MlpSmem::W1);
@@ -252,15 +283,15 @@ __global__ void __launch_bounds__(128) mlp_infer_kernel(const float *src, size_t
 
     // weights (already in operand layout) into shared memory
     for (int i = tid; i < kMlpHidden * kMlpIn; i += 128)
-        w1[i] = net->w1[i];
+        w1[i] = net.w1[i];
     for (int i = tid; i < kMlpHidden * kMlpHidden; i += 128)
-        w2[i] = net->w2[i];
+        w2[i] = net.w2[i];
     mbar_init_if(leader, bar);
     fence_mbar_init_if(leader);
     *flag = 0;
     __syncwarp();
     if (warp == 0)
-        tmem_alloc_warp(tmem_slot, 64);  // columns 0-31: layer 1, 32-63: layer 2
+        tmem_alloc_warp(tmem_slot, 32);  // 32 FP32 columns: layer 1, then layer 2
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     cta_sync();
@@ -273,32 +304,47 @@ __global__ void __launch_bounds__(128) mlp_infer_kernel(const float *src, size_t
     unsigned phase = 0;
 
     const size_t tiles = (N + 127) / 128;
-    for (size_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    // node values of the next tile are loaded while the current one computes
+    auto load = [&](size_t tile, float *v) {
         const size_t node = tile * 128 + tid;
-        const bool valid = node < N;
-        float f[kMlpIn];
-        if (valid) {
+        if (tile < tiles && node < N) {
             if constexpr (FROM_MOMENTS) {
-                float m[10];
 #pragma unroll
                 for (int k = 0; k < 10; k++)
-                    m[k] = src[size_t(k) * N + node];
-                node_features(m, net->r_ii, net->r_ij, f);
+                    v[k] = src[size_t(k) * N + node];
             } else {
 #pragma unroll
                 for (int k = 0; k < kMlpIn; k++)
-                    f[k] = src[node * kMlpIn + k];
+                    v[k] = src[node * kMlpIn + k];
             }
         } else {
 #pragma unroll
             for (int k = 0; k < kMlpIn; k++)
-                f[k] = 0.0f;
+                v[k] = 0.0f;
         }
-        const bool inside = valid && in_range(f, *net);
+    };
+    constexpr int NV = FROM_MOMENTS ? 10 : kMlpIn;
+    float next[kMlpIn];
+    load(blockIdx.x, next);
+    for (size_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const size_t node = tile * 128 + tid;
+        const bool valid = node < N;
+        float f[kMlpIn];
+        if constexpr (FROM_MOMENTS) {
+            node_features(next, net.r_ii, net.r_ij, f);
+        } else {
+#pragma unroll
+            for (int k = 0; k < kMlpIn; k++)
+                f[k] = next[k];
+        }
+        (void)NV;
+        load(tile + gridDim.x, next);
+        const bool inside = valid && in_range(f, net);
         // layer 1 operand: this thread's row of standardised features
 #pragma unroll
         for (int k = 0; k < kMlpIn; k++)
-            a1[umma_index(tid, k, 128)] = __float2half_rn((f[k] - net->in_mean[k]) * net->in_scale[k]);
+            f[k] = fmaf(f[k], net.in_scale[k], net.in_shift[k]);
+        store_row_f16<kMlpIn>(a1, tid, f);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         tc_fence_before();
         cta_sync();
@@ -315,8 +361,11 @@ __global__ void __launch_bounds__(128) mlp_infer_kernel(const float *src, size_t
         tmem_ld_32cols(tmem + lane_base, h);
 #pragma unroll
         for (int j = 0; j < kMlpHidden; j++)
-            a2[umma_index(tid, j, 128)] = __float2half_rn(gelu(h[j] + net->b1[j]));
+            h[j] = gelu_fast(h[j] + net.b1[j]);
+        store_row_f16<kMlpHidden>(a2, tid, h);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        // every thread has read its layer-1 accumulators (tcgen05.wait::ld):
+        // layer 2 may overwrite the same columns
         tc_fence_before();
         cta_sync();
         if (*flag)
@@ -325,7 +374,7 @@ __global__ void __launch_bounds__(128) mlp_infer_kernel(const float *src, size_t
         // layer 2: K = 32 as two K = 16 steps
 #pragma unroll
         for (int s = 0; s < 2; s++)
-            umma_f16_if(leader, tmem + kMlpHidden, umma_desc(a2 + s * 2 * (MlpSmem::LBO_A / 2), MlpSmem::LBO_A, MlpSmem::SBO),
+            umma_f16_if(leader, tmem, umma_desc(a2 + s * 2 * (MlpSmem::LBO_A / 2), MlpSmem::LBO_A, MlpSmem::SBO),
                         umma_desc(w2 + s * 2 * (MlpSmem::LBO_W / 2), MlpSmem::LBO_W, MlpSmem::SBO), idesc, s > 0);
         umma_commit_if(leader, bar);
         if (!mbar_wait_bounded(bar, phase, timeout_ns)) {
@@ -334,16 +383,16 @@ __global__ void __launch_bounds__(128) mlp_infer_kernel(const float *src, size_t
         }
         phase ^= 1u;
         tc_fence_after();
-        tmem_ld_32cols(tmem + lane_base + kMlpHidden, h);
-        float y = net->b3;
+        tmem_ld_32cols(tmem + lane_base, h);
+        float y = net.b3;
 #pragma unroll
         for (int j = 0; j < kMlpHidden; j++)
-            y = fmaf(net->w3[j], gelu(h[j] + net->b2[j]), y);
+            y = fmaf(net.w3[j], gelu_fast(h[j] + net.b2[j]), y);
         if (valid) {
             if constexpr (RAW_Y)
                 out[node] = y;
             else
-                out[node] = inside ? fminf(fmaxf(net->out_scale * y, net->dtau_lo), net->dtau_hi) : 0.0f;
+                out[node] = inside ? fminf(fmaxf(net.out_scale * y, net.dtau_lo), net.dtau_hi) : 0.0f;
         }
         tc_fence_before();
         cta_sync();
@@ -359,7 +408,7 @@ __global__ void __launch_bounds__(128) mlp_infer_kernel(const float *src, size_t
     cta_sync();
     tc_fence_after();
     if (warp == 0)
-        tmem_dealloc_warp(tmem, 64);
+        tmem_dealloc_warp(tmem, 32);
 }
 
 }  // namespace lbm

@@ -138,6 +138,10 @@ class Cavity:
         (an _lib.MLP) in every following step; None restores the plain method."""
         _lib.check(_lib.lib().lbm_closure_set(self._h, ctypes.byref(net) if net is not None else None))
 
+    def closure_refresh(self, every: int) -> None:
+        """Recompute the closure's dtau every `every` steps (1: every step)."""
+        _lib.check(_lib.lib().lbm_closure_refresh(self._h, int(every)))
+
     def closure_dtau(self) -> np.ndarray:
         nz, ny, nx = self.shape
         out = np.empty((nz, ny, nx), np.float32)

@@ -270,7 +270,7 @@ lbm_status lbm_batch_configure(lbm_batch *b, const lbm_batch_tuning *shape);
 /* ------------------------------------------------------ learned closure
  * A per-node network predicts a correction dtau to the relaxation time of
  * an under-resolved run; no counterpart in the reference.  Network: 16
- * features -> 32 -> 32 -> 1 with exact GELU.  Features of a node from its
+ * features -> 32 -> 32 -> 1 with GELU (tanh form).  Features of a node from its
  * stored moments m (rho-1, 3u, 3v, 3w, 4.5 m_aa, 9 m_ab): the 10 moments and
  * 3 (u_a u_b - m_ab) / (2 scale tau0) for ab = xx, xy, xz, yy, yz, zz, each
  * standardised as (f - in_mean) * in_scale.  dtau = clamp(out_scale * y,
@@ -305,8 +305,14 @@ typedef struct lbm_train_report {
  * interior node of the current state, from a counter-based hash of `seed`. */
 lbm_status lbm_perturb_velocity(lbm_handle *h, float amplitude, uint64_t seed);
 
-/* coarse state := 2:1 box filter of the fine state (mean of the 8 fine
- * nodes of every coarse node, all 10 stored moments; fine = 2 x coarse). */
+/* coarse state := 2:1 box filter of the fine state (fine = 2 x coarse in
+ * every direction; mean over the 8 fine nodes of every coarse node).  rho-1
+ * and the velocity are averaged; each second-order moment is the mean of its
+ * equilibrium part u_a u_b (so the subgrid stress mean(u_a u_b) - mean(u_a)
+ * mean(u_b) is kept) plus kappa times the mean of its non-equilibrium part,
+ * kappa = 2 (tau_c/tau_f) (1-omega_c)/(1-omega_f): the coarse lattice's
+ * non-equilibrium stress for the same flow (twice the strain rate per step
+ * at equal lattice velocity, its own tau and collision factor). */
 lbm_status lbm_filter_2to1(lbm_handle *fine, lbm_handle *coarse);
 
 /* Sample store for training, capacity in samples (16 features + 1 target). */
@@ -315,11 +321,14 @@ lbm_status lbm_trainer_destroy(lbm_trainer *t);
 
 /* Training pairs from one coarse step: `coarse` holds F(t) (a filtered fine
  * state) and is advanced one plain step by this call; `fine_next` is the
- * fine run two fine steps later.  For every `stride`-th interior node: the
- * features of F(t) and the dtau for which its collision gives the filtered
- * fine state instead (first order).  *total = samples stored so far. */
+ * fine run two fine steps later.  For every `stride`-th interior node whose
+ * post-step non-equilibrium second-order moments have an RMS (stored units)
+ * above `min_neq`: the features of F(t) and the dtau for which its collision
+ * gives the filtered fine state instead, to first order in dtau (the
+ * estimate is a ratio with that RMS in the denominator, hence the floor).
+ * *total = samples stored so far. */
 lbm_status lbm_trainer_add(lbm_trainer *t, lbm_handle *coarse, lbm_handle *fine_next, uint32_t stride,
-                           uint64_t *total);
+                           float min_neq, uint64_t *total);
 
 /* Copy stored samples [first, first+count) to the host (features [n][16],
  * targets [n]; either may be NULL); *total = samples stored. */
@@ -344,6 +353,10 @@ lbm_status lbm_mlp_infer(int32_t device, const lbm_mlp *net, const float *featur
 /* Use the network in every following lbm_step of this handle (NULL: back to
  * the plain collision).  FP32 storage, no function objects. */
 lbm_status lbm_closure_set(lbm_handle *h, const lbm_mlp *net);
+
+/* Recompute dtau every `every` steps (default 1: every step) and reuse it in
+ * between -- a lagged closure for runs where it varies slowly. */
+lbm_status lbm_closure_refresh(lbm_handle *h, int32_t every);
 
 /* The dtau field of the last closure step ([z][y][x], count = nodes). */
 lbm_status lbm_closure_dtau(lbm_handle *h, float *host, size_t count);

@@ -5,7 +5,8 @@ kernels (gradients) and the tensor-core inference against plain numpy.  It is
 not part of the product and is never executed on the product path.
 
 The network and features have no counterpart in the reference; they follow
-cudalbm_b200/csrc/lbm_mlp.cuh (16 -> 32 -> 32 -> 1, exact GELU, features =
+cudalbm_b200/csrc/lbm_mlp.cuh (16 -> 32 -> 32 -> 1, GELU in its tanh form
+0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))) (Hendrycks & Gimpel 2016), features =
 10 stored moments + 6 strain-rate components 3 (u_a u_b - m_ab) / (2 scale tau0),
 standardised as (f - in_mean) * in_scale).
 """
@@ -15,16 +16,17 @@ import math
 
 import numpy as np
 
-_ERF = np.vectorize(math.erf)
 WEIGHTS = ("w1", "b1", "w2", "b2", "w3", "b3")
+_A, _B = math.sqrt(2.0 / math.pi), 0.044715
 
 
 def gelu(z):
-    return 0.5 * z * (1.0 + _ERF(z / math.sqrt(2.0)))
+    return 0.5 * z * (1.0 + np.tanh(_A * (z + _B * z ** 3)))
 
 
 def gelu_grad(z):
-    return 0.5 * (1.0 + _ERF(z / math.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / math.sqrt(2.0 * math.pi)
+    t = np.tanh(_A * (z + _B * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * _A * (1.0 + 3.0 * _B * z * z)
 
 
 def params_of(mlp) -> dict:

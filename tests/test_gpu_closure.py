@@ -160,3 +160,17 @@ def test_training_lowers_the_loss(samples):
     assert rep["samples"] == len(tr) and rep["steps"] == 300
     assert rep["loss_last"] < rep["loss_first"]
     assert np.all(np.isfinite(np.array(net.w2)))
+
+
+def test_samples_and_training_are_reproducible():
+    tr1, _, _ = make_samples(q=19, n=32, steps=20, seed=5, snapshots=1)
+    tr2, _, _ = make_samples(q=19, n=32, steps=20, seed=5, snapshots=1)
+    f1, t1 = tr1.samples()
+    f2, t2 = tr2.samples()
+    assert np.array_equal(f1.view(np.uint32), f2.view(np.uint32))
+    assert np.array_equal(t1.view(np.uint32), t2.view(np.uint32))
+    n1, r1 = tr1.fit(steps=50, batch=1024, seed=3)
+    n2, r2 = tr2.fit(steps=50, batch=1024, seed=3)
+    assert np.array_equal(np.array(n1.w2), np.array(n2.w2)) and r1["loss_last"] == r2["loss_last"]
+    tr1.close()
+    tr2.close()
