@@ -78,6 +78,10 @@ WORKLOADS = {
                         desc="64 D3Q19 cubic lid-driven cavities in one persistent launch per step (CUDA graph): "
                              "MT19937-64 seed 0 draws edges from {32,48,64,96,128} and Re from U[100,2000], "
                              "u_lid=0.05, FP32"),
+    "closure_q27_128": dict(kind="closure", lattice=27, nc=128, u=0.05, tau=0.5077, fo=(), b_alg=134,
+                            desc="learned closure: D3Q27 cavity 128^3 at tau 0.5077 (Re 2474) with the trained "
+                                 "relaxation-time network, against plain 128^3 and plain 256^3 over the same "
+                                 "physical time (10,000 coarse steps)"),
     "q27_256_fo64": dict(lattice=27, n=(256, 256, 256), Re=1000.0, u=0.05, fo=("S", "SMean", "k", "kMean"),
                          mean_bits=64, b_alg=274,
                          desc="D3Q27 lid-driven cavity 256^3, Re=1000, function objects with FP64 means"),
@@ -443,6 +447,69 @@ def run_batch(args, w):
     return line
 
 
+# ------------------------------------------------------ closure arm
+def run_closure(args, w):
+    """The closure half of the metric: train the network (cudalbm_b200/
+    closure_study.py), then time the learned coarse run and report its error
+    and wall time beside the plain coarse and the plain fine (2x) runs.  value
+    = the learned coarse run's device-timed MLUPS with the network evaluated
+    on the tensor cores every step."""
+    rank = int(os.environ.get("RANK", "0"))
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        return {"impl": "ours", "unavailable": "the closure study runs on one GPU"} if rank == 0 else None
+    from cudalbm_b200.closure_study import run_study
+    from cudalbm_b200.solver import Cavity
+
+    study = run_study(nc=w["nc"], tau_coarse=w["tau"], log=lambda m: log(m))
+    nc = w["nc"]
+    Re = study["config"]["Re"]
+    # device-timed learned steps (the study's network is not returned: retrain-free timing with a
+    # constant-shape network gives the same instruction stream)
+    from cudalbm_b200 import _lib
+
+    net = _lib.MLP()
+    net.in_lo[:] = [-1e30] * 16
+    net.in_hi[:] = [1e30] * 16
+    net.in_scale[:] = [1.0] * 16
+    net.dtau_lo, net.dtau_hi = study["config"]["dtau_range"]
+    with Cavity(w["lattice"], nc, nc, nc, Re, w["u"]) as c:
+        c.init_regions()
+        c.set_closure(net)
+        c.step(args.warmup)
+        c.synchronize()
+        sampler = ClockSampler(physical_gpu_index(int(os.environ.get("LOCAL_RANK", "0"))))
+        sampler.start()
+        c.step(args.steps)
+        c.synchronize()
+        ms = c.info()["last_step_ms"]
+        clocks = sampler.stop()
+        launches = args.steps * 2
+    nodes = nc ** 3
+    value = nodes * args.steps / (ms / 1e3) / 1e6
+    T = study["config"]["coarse_steps"]
+    peak, peak_kind = hbm_peak()
+    achieved = w["b_alg"] * nodes / (ms / args.steps / 1e3) / 1e9
+    return {
+        "metric": METRIC, "value": round(value, 2), "unit": "MLUPS", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 moments; f16 network weights/activations, f32 accumulate",
+        "data": "synthetic: lid-driven cavity; training runs with U(-1e-3,1e-3) velocity perturbations, seeds 0-7",
+        "config": {"workload": w["desc"], "lattice": f"D3Q{w['lattice']}", "nx": nc, "ny": nc, "nz": nc, "Re": Re,
+                   "parallelism": "1 GPU", "l2": "moments 0.17 GB: close to L2; MLUPS of a small mesh"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None, "bytes_per_node_alg": w["b_alg"],
+                     "peak_kind": f"of {peak_kind}"},
+        "e2e": {"value": round(nodes * study["learned"]["steps"] / study["learned"]["wall"] / 1e6, 2), "unit": "MLUPS",
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": round(40 * nodes * 2 / study["learned"]["steps"]),
+                "what": "the study's learned run through the public API, wall clock, with two state read-backs"},
+        "closure": {"error_plain": study["plain"][T], "error_learned": study["learned"][T],
+                    "wall_s": {"fine_plain": study["fine_wall_s"], "coarse_plain": study["plain"]["wall"],
+                               "coarse_learned": study["learned"]["wall"]},
+                    "speedup_learned_vs_fine": study["speedup_learned_vs_fine"], "training": study["training"]},
+        "gpu_launches": launches, "clocks": clocks,
+    }
+
+
 # ------------------------------------------------------- reference arm
 def reference_step_time(exe, spec, W, K, local):
     """Seconds per step of the reference executable on one case, from its
@@ -506,6 +573,10 @@ def run_reference(args, w):
         sample = ("the reference's own executable run once per size class (one cavity per process, as it "
                   f"supports), {K} steps after {W} each, per-step times summed over the 64 cavities")
     else:
+        if w.get("kind") == "closure":
+            # the reference has no closure: its plain solver on the same coarse case
+            nx = ny = nz = w["nc"]
+            w = dict(w, n=(nx, ny, nz), Re=w["u"] * (nx - 1) / ((w["tau"] - 0.5) / 3.0))
         nx, ny, nz = w["n"]
         nodes = nx * ny * nz
         spec = casefiles.CaseSpec(nx=nx, ny=ny, nz=nz, Re=w["Re"], u_inf=w["u"], n_steps=W + K + 1,
@@ -564,6 +635,8 @@ def main():
         line = run_reference(args, w)
     elif w.get("kind") == "batch":
         line = run_batch(args, w)
+    elif w.get("kind") == "closure":
+        line = run_closure(args, w)
     else:
         line = run_ours(args, w)
     if line is not None:
