@@ -200,31 +200,11 @@ def cpu_baseline(w, budget_s: float = 12.0):
 def run_ours(args, w):
     import numpy as np
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
+    from cudalbm_b200.replicas import Replicas
 
-        import torch
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(v: float) -> float:
-        if dist is None:
-            return v
-        import torch
-
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    group = Replicas("nccl")
+    world, rank, local = group.world, group.rank, group.local
+    barrier, max_over_ranks = group.barrier, group.max
 
     from cudalbm_b200 import _lib
     from cudalbm_b200.solver import NVARS, Cavity
@@ -278,6 +258,7 @@ def run_ours(args, w):
     d2h = sum(b.array.nbytes for b in outs.values())
     red = {"mass": float(mon.array[-1]["mass"]), "nonfinite": int(mon.array["nonfinite"].max())}
     cav.close()
+    group.close()
 
     if rank != 0:
         return None

@@ -153,6 +153,20 @@ __global__ void cut_plane_kernel(float *out, const T *src, int nvars, int nx, in
     }
 }
 
+// Self-test of the failure path: every thread waits, with the step kernels'
+// bounded wait, on an mbarrier that nothing arrives on; the wait gives up
+// after timeout_ns and the fault is recorded as in the step kernels.  No
+// copy or other asynchronous operation is in flight.
+__global__ void wait_timeout_kernel(lbm::StepFault *fault, uint64_t timeout_ns)
+{
+    __shared__ __align__(8) uint64_t bar;
+    lbm::mbar_init_if(threadIdx.x == 0, &bar);
+    lbm::fence_mbar_init_if(threadIdx.x == 0);
+    __syncthreads();
+    if (!lbm::mbar_wait_bounded(&bar, 0u, timeout_ns))
+        lbm::record_fault(fault, lbm::ERR_TMA_TIMEOUT, -1, -1, 0, 0u, 0u, 0u, &bar);
+}
+
 template <typename ST>
 __global__ void reduce_kernel(const ST *m, size_t N, double *acc, unsigned long long *bad)
 {
@@ -942,6 +956,27 @@ lbm_status lbm_cut_plane(lbm_handle *h, lbm_field_set set, int32_t axis, float p
     LBM_CUDA(cudaMemcpyAsync(host_out, dst, total * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
     LBM_CUDA(cudaStreamSynchronize(h->stream));
     return LBM_OK;
+}
+
+lbm_status lbm_selftest_wait_timeout(int32_t device, uint64_t timeout_ns)
+{
+    if (timeout_ns == 0 || timeout_ns > 10000000000ull)
+        return fail(LBM_ERR_ARG, "lbm_selftest_wait_timeout: timeout must be in (0, 10 s]");
+    LBM_CUDA(cudaSetDevice(device));
+    lbm::StepFault *d = nullptr;
+    LBM_CUDA(cudaMalloc(&d, sizeof(*d)));
+    cudaMemset(d, 0, sizeof(*d));
+    wait_timeout_kernel<<<1, 64>>>(d, timeout_ns);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaDeviceSynchronize();
+    lbm::StepFault f{};
+    if (e == cudaSuccess)
+        e = cudaMemcpy(&f, d, sizeof(f), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess)
+        return fail(LBM_ERR_CUDA, std::string("lbm_selftest_wait_timeout: ") + cudaGetErrorString(e));
+    return lbm::check_fault(f, "the self-test wait");
 }
 
 lbm_status lbm_host_alloc(size_t bytes, void **out)

@@ -361,6 +361,13 @@ lbm_status lbm_closure_refresh(lbm_handle *h, int32_t every);
 /* The dtau field of the last closure step ([z][y][x], count = nodes). */
 lbm_status lbm_closure_dtau(lbm_handle *h, float *host, size_t count);
 
+/* Self-test of the device-side failure path: a kernel waits with the step
+ * kernels' bounded wait on an mbarrier that nothing arrives on; after
+ * timeout_ns the wait gives up, records where, and the call returns
+ * LBM_ERR_TIMEOUT with that record in lbm_last_error() -- the CUDA context
+ * stays usable.  Replaces: nothing (the reference's waits are unbounded). */
+lbm_status lbm_selftest_wait_timeout(int32_t device, uint64_t timeout_ns);
+
 /* Page-locked host memory for fast transfers (cudaMallocHost); free with
  * lbm_host_free.  Replaces: the reference's pinned host::array variant
  * (src/array/hostArray.cuh:66-140). */
