@@ -442,6 +442,8 @@ void destroy_handle(lbm_handle *h)
         if (p)
             cudaFree(p);
     delete h->mlp;
+    if (h->steps_graph)
+        cudaGraphExecDestroy(h->steps_graph);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->stream && h->own_stream)
@@ -764,6 +766,61 @@ lbm_status lbm_read_fields(lbm_handle *h, lbm_field_set set, void *host, size_t 
     return LBM_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Plain steps (no function objects, no closure) repeat their launch
+// parameters every two steps, so lbm_step replays a CUDA graph of
+// kGraphSteps of them, captured from buffer 0: one graph launch instead of
+// kGraphSteps kernel launches (the per-launch cost matters for small meshes).
+constexpr uint64_t kGraphSteps = 16;
+
+lbm_status ensure_steps_graph(lbm_handle *h)
+{
+    if (h->steps_graph)
+        return LBM_OK;
+    const int cur0 = h->cur;
+    const int64_t t0 = h->t;
+    const uint64_t l0 = h->launches;
+    h->cur = 0;
+    LBM_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    lbm_status s = LBM_OK;
+    for (uint64_t i = 0; i < kGraphSteps && s == LBM_OK; i++)
+        s = launch_step<float>(h);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    h->cur = cur0;
+    h->t = t0;
+    h->launches = l0;
+    if (s != LBM_OK) {
+        if (g)
+            cudaGraphDestroy(g);
+        return s;
+    }
+    if (e != cudaSuccess)
+        return fail(LBM_ERR_CUDA, std::string("step graph capture: ") + cudaGetErrorString(e));
+    const cudaError_t ei = cudaGraphInstantiate(&h->steps_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+        h->steps_graph = nullptr;
+        return fail(LBM_ERR_CUDA, std::string("step graph instantiation: ") + cudaGetErrorString(ei));
+    }
+    return LBM_OK;
+}
+
+void drop_steps_graph(lbm_handle *h)
+{
+    if (h->steps_graph) {
+        cudaGraphExecDestroy(h->steps_graph);
+        h->steps_graph = nullptr;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
 lbm_status lbm_step(lbm_handle *h, uint64_t n)
 {
     if (!h)
@@ -771,9 +828,30 @@ lbm_status lbm_step(lbm_handle *h, uint64_t n)
     LBM_CUDA(cudaSetDevice(h->cfg.device));
     if (n == 0)
         return LBM_OK;
-    LBM_CUDA(cudaEventRecord(h->ev0, h->stream));
     const bool md = h->cfg.mean_bits == 64;
-    for (uint64_t i = 0; i < n; i++) {
+    const bool graphed = !h->cfg.function_objects && !h->closure && n >= kGraphSteps;
+    if (graphed) {
+        // built once per kernel variant, outside the timed span
+        lbm_status s = ensure_steps_graph(h);
+        if (s != LBM_OK)
+            return s;
+    }
+    LBM_CUDA(cudaEventRecord(h->ev0, h->stream));
+    uint64_t i = 0;
+    if (graphed) {
+        lbm_status s;
+        if (h->cur != 0) {
+            if ((s = launch_step<float>(h)) != LBM_OK)
+                return s;
+            i++;
+        }
+        for (; n - i >= kGraphSteps; i += kGraphSteps) {
+            LBM_CUDA(cudaGraphLaunch(h->steps_graph, h->stream));
+            h->t += int64_t(kGraphSteps);
+            h->launches += kGraphSteps;
+        }
+    }
+    for (; i < n; i++) {
         lbm_status s = md ? launch_step<double>(h) : launch_step<float>(h);
         if (s != LBM_OK)
             return s;
@@ -1072,6 +1150,7 @@ lbm_status apply_variant(lbm_handle *h, int tx, int ty, int stages, int npb, int
         LBM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(l.smem)));
     h->launcher = l;
     h->zc = std::max(1, std::min<int>(zc, int(h->cfg.nz)));
+    drop_steps_graph(h);
     for (int b = 0; b < 2; b++) {
         lbm_status s = make_tmap(h, b);
         if (s != LBM_OK)

@@ -47,6 +47,7 @@ struct lbm_handle {
     bool closure = false;
     float *dtau = nullptr;             // [N] relaxation-time correction of the current step
     lbm::MlpDevice *mlp = nullptr;     // network for the closure (host copy, passed by value)
+    cudaGraphExec_t steps_graph = nullptr;  // kGraphSteps plain steps from buffer 0 (see lbm_step)
     int closure_every = 1;             // recompute dtau every this many steps
     uint64_t closure_steps = 0;        // closure steps taken since lbm_closure_set
 };
