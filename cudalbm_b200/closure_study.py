@@ -2,7 +2,8 @@
 coarse grid, with and without the learned relaxation-time correction, judged
 by a fine run at twice the resolution.
 
-    python -m cudalbm_b200.closure_study [--nc 128] [--coarse-steps 10000] [--json out.json]
+    python -m cudalbm_b200.closure_study [--nc 128] [--coarse-steps 10000] [--seeds 8]
+        [--snapshots 6] [--stride 3] [--json out.json]
 
 Steps (all on the GPU through the library):
  1. Training data: ``seeds`` fine runs (2 nc per edge) of the lid-driven
@@ -51,6 +52,27 @@ def centreline(m: np.ndarray) -> np.ndarray:
     return 0.25 * (m[1, lo, :, lo] + m[1, lo, :, hi] + m[1, hi, :, lo] + m[1, hi, :, hi]) / 3.0
 
 
+def centreline_at_coarse_nodes(fine: Cavity, nc: int) -> np.ndarray:
+    """``centreline`` of the fine run sampled at the coarse nodes' positions
+    (trilinear): two device cut planes at the coarse middle z positions,
+    interpolated in x and y here -- no full read of the fine field."""
+    nf = fine.shape[0]
+    lo, hi = (nc - 1) // 2, nc // 2
+    y = np.arange(nc) * (nf - 1) / (nc - 1)
+    j0 = np.minimum(np.floor(y).astype(int), nf - 2)
+    wy = y - j0
+    cols = []
+    for k in (lo, hi):
+        u = fine.cut_plane(2, k / (nc - 1))[1].astype(np.float64)  # [ny][nx] at z of coarse plane k
+        for i in (lo, hi):
+            x = i * (nf - 1) / (nc - 1)
+            i0 = min(int(np.floor(x)), nf - 2)
+            wx = x - i0
+            ux = u[:, i0] * (1 - wx) + u[:, i0 + 1] * wx
+            cols.append(ux[j0] * (1 - wy) + ux[j0 + 1] * wy)
+    return 0.25 * sum(cols) / 3.0
+
+
 def sample_at_coarse_nodes(fine_vel: np.ndarray, nc: int) -> np.ndarray:
     """Fine velocity [3][nf][nf][nf] at the coarse node positions (trilinear)."""
     nf = fine_vel.shape[1]
@@ -74,18 +96,25 @@ def run_study(nc: int = 128, lattice: int = 27, u_lid: float = 0.05, tau_coarse:
               coarse_steps: int = 10000, seeds: int = 8, snapshots: int = 6, stride: int = 3,
               min_neq: float = 3e-4, train_steps: int = 3000, batch: int = 16384, lr: float = 2e-3,
               dtau_range: Sequence[float] = (0.0, 0.05), shrink: Sequence[float] = (1.0, 0.5, 0.25),
-              device: int = 0, save: str = "", log: Callable[[str], None] = print) -> Dict[str, object]:
+              device: int = 0, save: str = "", field_pos_max: int = 512,
+              log: Callable[[str], None] = print) -> Dict[str, object]:
+    """``field_pos_max``: largest fine edge for which the whole fine field is
+    read back to sample it at the coarse nodes (field_pos); above it only
+    the centreline is sampled (two device cut planes)."""
     nf = 2 * nc
     Re = u_lid * (nc - 1) / ((tau_coarse - 0.5) / 3.0)
     Tc, Tf = int(coarse_steps), 2 * int(coarse_steps)
     snaps = [int(Tf * (k + 1) / (snapshots + 1)) for k in range(snapshots)]
     cav = lambda n: Cavity(lattice, n, n, n, Re, u_lid, device=device)
+    whole_field = nf <= field_pos_max
 
     def fine_run(seed, trainer=None, judge_at=()):
         """Fine run to Tf; samples at the snapshots, filtered states at judge_at."""
         out = {}
         with cav(nf) as f, cav(nc) as c:
             f.init_regions()
+            if nf >= 512:
+                f.autotune(3)
             if seed is not None:
                 f.perturb_velocity(1e-3, seed)
             f.synchronize()
@@ -96,7 +125,8 @@ def run_study(nc: int = 128, lattice: int = 27, u_lid: float = 0.05, tau_coarse:
                 done = s
                 if s in judge_at:
                     c.filter_from(f)
-                    out[s // 2] = (c.read(), sample_at_coarse_nodes(f.read()[1:4], nc))
+                    out[s // 2] = (c.read(), centreline_at_coarse_nodes(f, nc),
+                                   sample_at_coarse_nodes(f.read()[1:4], nc) if whole_field else None)
                 if trainer is not None and s in snaps:
                     c.filter_from(f)
                     f.step(2)
@@ -107,7 +137,7 @@ def run_study(nc: int = 128, lattice: int = 27, u_lid: float = 0.05, tau_coarse:
             out["wall"] = time.perf_counter() - t0
         return out
 
-    def coarse_run(net, judge, times=(Tc // 2, Tc)):
+    def coarse_run(net, judge, times=(Tc // 2, Tc), dtau=False):
         res = {}
         with cav(nc) as c:
             c.init_regions()
@@ -124,13 +154,17 @@ def run_study(nc: int = 128, lattice: int = 27, u_lid: float = 0.05, tau_coarse:
                 walls = time.perf_counter() - t0
                 done = t
                 m = c.read()
-                jb, ji = judge[t]
+                jb, jc, ji = judge[t]
                 res[t] = {"centreline_box": rel(centreline(m), centreline(jb)),
                           "field_box": rel(m[1:4], jb[1:4]),
-                          "centreline_pos": rel(centreline(m), centreline(np.concatenate([m[:1], ji, m[4:]]))),
-                          "field_pos": rel(m[1:4], ji)}
+                          "centreline_pos": rel(centreline(m), jc),
+                          "field_pos": rel(m[1:4], ji) if ji is not None else None}
             res["wall"] = walls
             res["steps"] = Tc - 2
+            if dtau:
+                dt = c.closure_dtau()
+                res["dtau"] = {"mean": float(dt.mean()), "max": float(dt.max()),
+                               "nonzero_fraction": float((dt != 0).mean())}
         return res
 
     t0 = time.perf_counter()
@@ -164,12 +198,7 @@ def run_study(nc: int = 128, lattice: int = 27, u_lid: float = 0.05, tau_coarse:
 
     judge = fine_run(None, judge_at=(Tf // 2, Tf))
     plain = coarse_run(None, judge)
-    learned = coarse_run(net, judge)
-    with cav(nc) as c:  # fraction of the evaluation state inside the training range
-        c.init_regions()
-        c.set_closure(net)
-        c.step(Tc)
-        dt = c.closure_dtau()
+    learned = coarse_run(net, judge, dtau=True)
     if save:
         save_mlp(save, net)
     out = {
@@ -182,7 +211,7 @@ def run_study(nc: int = 128, lattice: int = 27, u_lid: float = 0.05, tau_coarse:
         "plain": plain, "learned": learned,
         "fine_wall_s": judge["wall"],
         "speedup_learned_vs_fine": judge["wall"] / learned["wall"],
-        "dtau": {"mean": float(dt.mean()), "max": float(dt.max()), "nonzero_fraction": float((dt != 0).mean())},
+        "dtau": learned.pop("dtau"),
     }
     for t in (Tc // 2, Tc):
         log(f"t={t}: plain {plain[t]}  learned {learned[t]}")
@@ -196,10 +225,18 @@ def main():
     ap.add_argument("--coarse-steps", type=int, default=10000)
     ap.add_argument("--seeds", type=int, default=8)
     ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--snapshots", type=int, default=6)
+    ap.add_argument("--stride", type=int, default=3, help="every stride-th interior node is a sample")
+    ap.add_argument("--dtau-range", default="0,0.05", help="clip of the targets and of the output, lo,hi")
+    ap.add_argument("--shrink", default="1,0.5,0.25", help="output scale factors tried in the calibration "
+                    "(0 = the plain method)")
     ap.add_argument("--save", default="", help="write the trained network (.npz)")
     ap.add_argument("--json", default="", help="write the results")
     a = ap.parse_args()
-    res = run_study(nc=a.nc, coarse_steps=a.coarse_steps, seeds=a.seeds, train_steps=a.train_steps, save=a.save)
+    res = run_study(nc=a.nc, coarse_steps=a.coarse_steps, seeds=a.seeds, train_steps=a.train_steps,
+                    snapshots=a.snapshots, stride=a.stride, save=a.save,
+                    dtau_range=[float(v) for v in a.dtau_range.split(",")],
+                    shrink=[float(v) for v in a.shrink.split(",")])
     text = json.dumps(res, indent=1, default=float)
     if a.json:
         with open(a.json, "w") as fh:

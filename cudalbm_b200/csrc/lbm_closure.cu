@@ -910,6 +910,8 @@ lbm_status lbm_closure_set(lbm_handle *h, const lbm_mlp *net)
     }
     if (h->cfg.function_objects || h->storage != LBM_STORAGE_F32)
         return fail(LBM_ERR_ARG, "lbm_closure_set: the closure runs with FP32 storage and no function objects");
+    if (!(net->dtau_lo <= net->dtau_hi) || !(h->tau + net->dtau_lo > 0.5f))
+        return fail(LBM_ERR_ARG, "lbm_closure_set: need dtau_lo <= dtau_hi and tau + dtau_lo > 0.5");
     void *fn;
     size_t smem;
     if (!pick_closure(h->Q, h->launcher.tx, h->launcher.ty, h->launcher.stages, h->launcher.pop_buffers, fn, smem)) {

@@ -351,7 +351,9 @@ lbm_status lbm_mlp_infer(int32_t device, const lbm_mlp *net, const float *featur
                          int32_t tensor_cores);
 
 /* Use the network in every following lbm_step of this handle (NULL: back to
- * the plain collision).  FP32 storage, no function objects. */
+ * the plain collision).  FP32 storage, no function objects; LBM_ERR_ARG
+ * unless dtau_lo <= dtau_hi and tau + dtau_lo > 0.5 (a positive viscosity
+ * at every node). */
 lbm_status lbm_closure_set(lbm_handle *h, const lbm_mlp *net);
 
 /* Recompute dtau every `every` steps (default 1: every step) and reuse it in

@@ -174,3 +174,18 @@ def test_samples_and_training_are_reproducible():
     assert np.array_equal(np.array(n1.w2), np.array(n2.w2)) and r1["loss_last"] == r2["loss_last"]
     tr1.close()
     tr2.close()
+
+
+def test_closure_range_must_keep_the_viscosity_positive():
+    net = _lib.MLP()
+    net.in_scale[:] = [1.0] * 16
+    with Cavity(19, 16, 16, 16, 300.0, 0.05) as c:
+        tau = c.info()["tau"]
+        net.dtau_lo, net.dtau_hi = 0.5 - tau, 0.01  # tau + dtau_lo = 0.5
+        with pytest.raises(RuntimeError, match="tau \\+ dtau_lo > 0.5"):
+            c.set_closure(net)
+        net.dtau_lo, net.dtau_hi = 0.02, 0.01
+        with pytest.raises(RuntimeError, match="dtau_lo <= dtau_hi"):
+            c.set_closure(net)
+        net.dtau_lo = 0.5 - tau + 1e-3
+        c.set_closure(net)
