@@ -41,6 +41,7 @@ import statistics
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -515,6 +516,7 @@ def reference_step_time(exe, spec, W, K, local):
         stamps = {}
         tail = []
         clocks = None
+        starter = None
         for line in proc.stdout:
             now = time.perf_counter()
             tail = (tail + [line])[-20:]
@@ -522,10 +524,16 @@ def reference_step_time(exe, spec, W, K, local):
                 t = int(line.split()[1])
                 stamps[t] = now
                 if t == W:
-                    sampler.start()
+                    # started aside: reading (and stamping) the step lines never waits on the sampler
+                    starter = threading.Thread(target=sampler.start)
+                    starter.start()
                 if t == W + K:
+                    starter.join()
                     clocks = sampler.stop()
         rc = proc.wait()
+        if starter is not None and clocks is None:
+            starter.join()
+            sampler.stop()
     if rc != 0 or W not in stamps or W + K not in stamps:
         return None, None, f"reference exited {rc}: {''.join(tail)[-300:]!r}"
     return (stamps[W + K] - stamps[W]) / K, clocks, None
