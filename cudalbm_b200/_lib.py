@@ -36,7 +36,7 @@ EXPORTS = ("lbm_config_default", "lbm_create", "lbm_destroy", "lbm_init_regions"
            "lbm_vts_write", "lbm_perturb_velocity", "lbm_filter_2to1", "lbm_trainer_create", "lbm_trainer_destroy",
            "lbm_trainer_add", "lbm_trainer_samples", "lbm_trainer_fit", "lbm_trainer_gradient", "lbm_mlp_infer",
            "lbm_closure_set", "lbm_closure_dtau", "lbm_closure_refresh",
-           "lbm_selftest_wait_timeout")
+           "lbm_selftest_wait_timeout", "lbm_field_statistics")
 
 
 class Config(ctypes.Structure):
@@ -172,6 +172,8 @@ def lib() -> ctypes.CDLL:
         L.lbm_closure_dtau.argtypes = [vp, vp, sz]
         L.lbm_closure_refresh.argtypes = [vp, i32]
         L.lbm_selftest_wait_timeout.argtypes = [i32, u64]
+        L.lbm_field_statistics.argtypes = [i32, vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, i32, i32, vp, vp,
+                                           vp]
         L.lbm_lbmbin_write.argtypes = [ctypes.c_char_p, u64, u64, u64, i32, ctypes.POINTER(ctypes.c_char_p), vp, u64,
                                        i32]
         for name in ("lbm_create", "lbm_destroy", "lbm_init_regions", "lbm_write_fields", "lbm_read_fields",
@@ -182,7 +184,8 @@ def lib() -> ctypes.CDLL:
                      "lbm_cut_plane", "lbm_vts_write", "lbm_perturb_velocity", "lbm_filter_2to1",
                      "lbm_trainer_create", "lbm_trainer_destroy", "lbm_trainer_add", "lbm_trainer_samples",
                      "lbm_trainer_fit", "lbm_trainer_gradient", "lbm_mlp_infer", "lbm_closure_set",
-                     "lbm_closure_dtau", "lbm_closure_refresh", "lbm_selftest_wait_timeout"):
+                     "lbm_closure_dtau", "lbm_closure_refresh", "lbm_selftest_wait_timeout",
+                     "lbm_field_statistics"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib

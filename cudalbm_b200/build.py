@@ -8,6 +8,7 @@ Outputs:
   cudalbm_b200/bin/momentBasedD3Q19    solver executables with the reference's
   cudalbm_b200/bin/momentBasedD3Q27    command line and case files
   cudalbm_b200/bin/fieldConvert        .LBMBin -> VTS (whole fields or cut planes)
+  cudalbm_b200/bin/fieldCalculate      containsNaN / spatialMean of saved times (on the GPU)
 """
 from __future__ import annotations
 
@@ -29,7 +30,7 @@ NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-cudart"
               "-I" + INCLUDE, "-I" + CSRC] + ARCH
 
 LIB_SOURCES = ["lbm_capi.cu", "lbm_batch.cu", "lbm_closure.cu", "variants_q19_f32.cu", "variants_q27_f32.cu", "variants_f16.cu", "variants_bf16.cu",
-               "lbm_noalloc.cu", "casefile.cpp", "lbmbin.cpp", "postprocess.cpp"]
+               "lbm_noalloc.cu", "lbm_fieldcalc.cu", "casefile.cpp", "lbmbin.cpp", "postprocess.cpp"]
 
 
 def _nvcc() -> str:
@@ -86,8 +87,8 @@ def _cxx() -> str:
 
 
 def build_executables(force: bool = False) -> list:
-    """momentBasedD3Q19 / momentBasedD3Q27 (host C++ over the library) and
-    fieldConvert."""
+    """momentBasedD3Q19 / momentBasedD3Q27 and fieldCalculate (host C++ over
+    the library) and fieldConvert (host only)."""
     out = []
     main = os.path.join(CSRC, "solver_main.cpp")
     os.makedirs(BIN, exist_ok=True)
@@ -98,6 +99,12 @@ def build_executables(force: bool = False) -> list:
             _run([_cxx(), "-std=c++17", "-O2", "-Wall", "-I" + INCLUDE, "-I" + CSRC, f"-DLBM_LATTICE={q}", main] + host +
                  ["-o", exe, "-L" + os.path.dirname(LIB), "-llbm_b200", "-Wl,-rpath,$ORIGIN/../lib"])
         out.append(exe)
+    # fieldCalculate: host C++ over the library (the reductions run on the GPU)
+    exe = os.path.join(BIN, "fieldCalculate")
+    if force or _stale(exe, _deps() + [LIB]):
+        _run([_cxx(), "-std=c++17", "-O2", "-Wall", "-I" + INCLUDE, "-I" + CSRC, os.path.join(CSRC, "fieldcalculate_main.cpp")]
+             + host + ["-o", exe, "-L" + os.path.dirname(LIB), "-llbm_b200", "-Wl,-rpath,$ORIGIN/../lib"])
+    out.append(exe)
     # fieldConvert: host only (no GPU, no library)
     exe = os.path.join(BIN, "fieldConvert")
     srcs = [os.path.join(CSRC, s) for s in ("fieldconvert_main.cpp", "casefile.cpp", "lbmbin.cpp", "postprocess.cpp")]

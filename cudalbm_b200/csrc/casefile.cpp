@@ -4,8 +4,11 @@
 #include <algorithm>
 #include <cctype>
 #include <charconv>
+#include <ctime>
 #include <filesystem>
 #include <fstream>
+#include <iomanip>
+#include <iostream>
 #include <sstream>
 
 #include "lbm_b200.h"
@@ -300,6 +303,61 @@ std::vector<uint64_t> time_indices(const std::string &dir, const std::string &pr
     }
     std::sort(out.begin(), out.end());
     return out;
+}
+
+void print_program_control(const ProgramControl &pc, const std::string &program, const std::vector<int> &devices,
+                           uint64_t latest)
+{
+    const std::time_t now = std::time(nullptr);
+    std::cout << "programControl:\n{\n"
+              << "    programName: " << program << ";\n"
+              << "    launchTime: " << std::put_time(std::localtime(&now), "%Y-%m-%d %H:%M:%S") << ";\n"
+              << "    launchDirectory: " << fs::current_path().string() << ";\n"
+              << "    deviceList: [";
+    for (size_t i = 0; i < devices.size(); i++)
+        std::cout << devices[i] << (i + 1 < devices.size() ? ", " : "");
+    std::cout << "];\n    caseName: " << pc.caseName << ";\n    Re = " << pc.Re << ";\n    nTimeSteps = " << pc.nTimeSteps
+              << ";\n    saveInterval = " << pc.saveInterval << ";\n    infoInterval = " << pc.infoInterval
+              << ";\n    latestTime = " << latest << ";\n    scalarType: 32 bit;\n    labelType: uint64_t;\n};\n"
+              << std::endl;
+}
+
+void print_lattice_mesh(const LatticeMesh &mesh)
+{
+    std::cout << "latticeMesh:\n{\n    nx = " << mesh.nx << ";\n    ny = " << mesh.ny << ";\n    nz = " << mesh.nz
+              << ";\n    Lx = " << mesh.Lx << ";\n    Ly = " << mesh.Ly << ";\n    Lz = " << mesh.Lz << ";\n};\n"
+              << std::endl;
+}
+
+std::vector<int> parse_gpu_list(int argc, char **argv, bool required)
+{
+    const std::string exe = fs::path(argv[0]).filename().string();
+    for (int i = 1; i < argc; i++) {
+        if (std::string(argv[i]) != "-GPU")
+            continue;
+        if (i + 1 >= argc)
+            throw CaseError("Input argument -GPU has not been supplied with a value; the correct syntax is -GPU 0,1 for example");
+        std::vector<int> ids;
+        std::string s = argv[i + 1], cur;
+        for (char c : s + ",") {
+            if (c == ',') {
+                if (!cur.empty()) {
+                    if (!is_number(cur) || cur.find('.') != std::string::npos)
+                        throw CaseError("-GPU is not numeric");
+                    ids.push_back(std::stoi(cur));
+                }
+                cur.clear();
+            } else {
+                cur.push_back(c);
+            }
+        }
+        if (ids.empty())
+            throw CaseError("-GPU is not numeric");
+        return ids;
+    }
+    if (!required)
+        return {0};
+    throw CaseError("Error: The -GPU argument is mandatory for the " + exe + " executable.");
 }
 
 }  // namespace lbm

@@ -60,4 +60,15 @@ uint32_t read_function_objects(const std::string &dir);
 // Time indices of <prefix>_<n>.LBMBin files in dir, sorted (fileIO.cuh:98-233).
 std::vector<uint64_t> time_indices(const std::string &dir, const std::string &prefix);
 
+// The programControl and latticeMesh blocks every reference executable prints
+// on start-up (programControl.cuh:86-120 without its banner, latticeMesh.cuh:95-104);
+// latestTime = the last saved time of the case (0 if none).
+void print_program_control(const ProgramControl &pc, const std::string &program, const std::vector<int> &devices,
+                           uint64_t latest);
+void print_lattice_mesh(const LatticeMesh &mesh);
+
+// -GPU <ids> of the command line ("0,1"); `required` as for the solvers,
+// else device 0 when absent (the post-processors, inputControl.cuh:204-226).
+std::vector<int> parse_gpu_list(int argc, char **argv, bool required);
+
 }  // namespace lbm

@@ -12,8 +12,9 @@
 // postProcess/<prefix>CutPlane_<d>=<c>_<t>.vts holding the plane (a mesh one
 // node thick).  The files match the reference's byte for byte, including its
 // cut-plane interpolation weight (see postprocess.hpp).  Other -fileType
-// values of the reference (vtu, tecplot) are not provided.  -GPU is accepted
-// and ignored: nothing here runs on a GPU.
+// values of the reference (vtu, tecplot) are not provided.  The start-up
+// blocks (programControl, latticeMesh) are printed as the solvers print them.
+// -GPU is optional (device 0) and only printed: nothing here runs on a GPU.
 #include <cstdio>
 #include <filesystem>
 #include <iostream>
@@ -41,6 +42,8 @@ const std::map<std::string, std::vector<std::string>> kFieldComponents = {
     {"kMean", {"kMean"}}};
 
 struct Args {
+    std::string program;
+    std::vector<int> gpus;
     std::vector<std::string> v;
     bool present(const std::string &name) const
     {
@@ -90,7 +93,10 @@ void report_write(const std::string &file, uint64_t bytes, bool dir_existed)
 int run(const Args &args)
 {
     const lbm::ProgramControl pc = lbm::read_program_control(".");
+    const std::vector<uint64_t> saved = lbm::time_indices(".", pc.caseName);
+    lbm::print_program_control(pc, args.program, args.gpus, saved.empty() ? 0 : saved.back());
     const lbm::LatticeMesh mesh = lbm::read_lattice_mesh(".");
+    lbm::print_lattice_mesh(mesh);
     const bool custom = args.present("-fieldName");
     const std::string prefix = custom ? args.value("-fieldName") : pc.caseName;
     std::vector<std::string> names = kMoments;
@@ -152,9 +158,11 @@ int run(const Args &args)
 int main(int argc, char **argv)
 {
     Args args;
+    args.program = argv[0];
     for (int i = 1; i < argc; i++)
         args.v.emplace_back(argv[i]);
     try {
+        args.gpus = lbm::parse_gpu_list(argc, argv, false);
         return run(args);
     } catch (const std::exception &e) {
         std::cerr << fs::path(argv[0]).filename().string() << ": " << e.what() << std::endl;

@@ -47,35 +47,6 @@ void check(lbm_status s)
         throw Failure{int(s), std::string(lbm_status_string(s)) + ": " + lbm_last_error()};
 }
 
-std::vector<int> parse_gpu_list(int argc, char **argv)
-{
-    const std::string exe = std::filesystem::path(argv[0]).filename().string();
-    for (int i = 1; i < argc; i++) {
-        if (std::string(argv[i]) != "-GPU")
-            continue;
-        if (i + 1 >= argc)
-            throw lbm::CaseError("Input argument -GPU has not been supplied with a value; the correct syntax is -GPU 0,1 for example");
-        std::vector<int> ids;
-        std::string s = argv[i + 1], cur;
-        for (char c : s + ",") {
-            if (c == ',') {
-                if (!cur.empty()) {
-                    if (!lbm::is_number(cur) || cur.find('.') != std::string::npos)
-                        throw lbm::CaseError("-GPU is not numeric");
-                    ids.push_back(std::stoi(cur));
-                }
-                cur.clear();
-            } else {
-                cur.push_back(c);
-            }
-        }
-        if (ids.empty())
-            throw lbm::CaseError("-GPU is not numeric");
-        return ids;
-    }
-    throw lbm::CaseError("Error: The -GPU argument is mandatory for the " + exe + " executable.");
-}
-
 void print_velocity_set()
 {
     static const int cx[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1};
@@ -153,28 +124,14 @@ std::string hms(long long s)
 
 int run(int argc, char **argv)
 {
-    const std::vector<int> gpus = parse_gpu_list(argc, argv);
+    const std::vector<int> gpus = lbm::parse_gpu_list(argc, argv, true);
     const lbm::ProgramControl pc = lbm::read_program_control(".");
     const std::vector<uint64_t> times = lbm::time_indices(".", pc.caseName);
     const uint64_t latest = times.empty() ? 0 : times.back();
 
-    const std::time_t now = std::time(nullptr);
-    std::cout << "programControl:\n{\n"
-              << "    programName: " << argv[0] << ";\n"
-              << "    launchTime: " << std::put_time(std::localtime(&now), "%Y-%m-%d %H:%M:%S") << ";\n"
-              << "    launchDirectory: " << std::filesystem::current_path().string() << ";\n"
-              << "    deviceList: [";
-    for (size_t i = 0; i < gpus.size(); i++)
-        std::cout << gpus[i] << (i + 1 < gpus.size() ? ", " : "");
-    std::cout << "];\n    caseName: " << pc.caseName << ";\n    Re = " << pc.Re << ";\n    nTimeSteps = " << pc.nTimeSteps
-              << ";\n    saveInterval = " << pc.saveInterval << ";\n    infoInterval = " << pc.infoInterval
-              << ";\n    latestTime = " << latest << ";\n    scalarType: 32 bit;\n    labelType: uint64_t;\n};\n"
-              << std::endl;
-
+    lbm::print_program_control(pc, argv[0], gpus, latest);
     const lbm::LatticeMesh mesh = lbm::read_lattice_mesh(".");
-    std::cout << "latticeMesh:\n{\n    nx = " << mesh.nx << ";\n    ny = " << mesh.ny << ";\n    nz = " << mesh.nz
-              << ";\n    Lx = " << mesh.Lx << ";\n    Ly = " << mesh.Ly << ";\n    Lz = " << mesh.Lz << ";\n};\n"
-              << std::endl;
+    lbm::print_lattice_mesh(mesh);
     if (mesh.nx % 8 || mesh.ny % 8 || mesh.nz % 8 || !mesh.nx || !mesh.ny || !mesh.nz)
         throw lbm::CaseError("block::nx() * mesh.nxBlocks() not equal to mesh.nx()\nMesh dimensions should be multiples of 8");
     print_velocity_set();

@@ -203,6 +203,24 @@ def write_vts(path: str, fields: np.ndarray, names: Iterable[str], lengths=(1.0,
     _lib.check(_lib.lib().lbm_vts_write(path.encode(), nx, ny, nz, L, nv, arr, fields.ctypes.data))
 
 
+def field_statistics(fields: np.ndarray, shape=None, tiled: bool = False, device: int = 0):
+    """fieldCalculate's checks of fields [nfields][nz][ny][nx] (or
+    [nfields][nodes] in the .LBMBin tiled order with tiled=True and
+    shape=(nz, ny, nx)), on the GPU: (NaN count, the reference's spatial mean
+    -- left-to-right float sum in global order / float(nodes) --, FP64 mean)
+    per field."""
+    fields = np.ascontiguousarray(fields, dtype=np.float32)
+    nf = fields.shape[0]
+    nz, ny, nx = shape if shape is not None else fields.shape[1:]
+    nan = np.zeros(nf, np.int32)
+    mean_ref = np.zeros(nf, np.float32)
+    mean = np.zeros(nf, np.float64)
+    _lib.check(_lib.lib().lbm_field_statistics(int(device), fields.ctypes.data, int(nx), int(ny), int(nz), int(nf),
+                                               _lib.ORDER_TILED if tiled else _lib.ORDER_GLOBAL, nan.ctypes.data,
+                                               mean_ref.ctypes.data, mean.ctypes.data))
+    return nan, mean_ref, mean
+
+
 class Batch:
     """Many independent cavities advanced by one persistent launch per step.
 

@@ -200,6 +200,22 @@ lbm_status lbm_autotune(lbm_handle *h, int32_t trial_steps, lbm_tuning *out);
  * No counterpart in the reference, which has no allocation-free entry point. */
 lbm_status lbm_reduce_moments_noalloc(const float *moments, uint64_t nodes, double out[3], void *stream);
 
+/* fieldCalculate -calculationType containsNaN / spatialMean for one saved
+ * time, on the GPU `device`: `fields` is host memory holding `nfields`
+ * fields of nx*ny*nz floats each, in `order` (LBM_ORDER_TILED: as stored in
+ * an .LBMBin file).  Per field k: nan_count[k] = number of NaN values
+ * (saturating at INT32_MAX; infinities are not NaN); mean_ref[k] = the
+ * reference's spatial mean -- the float sum of the values in global node
+ * order, added left to right from 0, divided by float(nodes) -- bit for bit;
+ * mean[k] = the FP64 sum of the non-NaN values (fixed summation order)
+ * divided by the node count.
+ * Copies the fields to a temporary device buffer.  Replaces: the host loops
+ * containsNaN and spatialMean of applications/fieldCalculate/
+ * fieldCalculate.cuh:74-170 (with fileInput.cuh:777-820's de-interleave). */
+lbm_status lbm_field_statistics(int32_t device, const float *fields, int64_t nx, int64_t ny, int64_t nz,
+                                int32_t nfields, lbm_order order, int32_t *nan_count, float *mean_ref,
+                                double *mean);
+
 /* -------------------------------------------------------------- batches
  * Many independent cavities advanced together.  Every step is ONE launch of a
  * persistent kernel (as many CTAs as fit on the GPU) whose CTAs take work
