@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <random>
 #include <string>
 #include <vector>
@@ -378,17 +379,22 @@ __global__ void forward_kernel(const float *feat, uint64_t n, const MlpParams *p
 // ------------------------------------------------------------- helpers
 MlpDevice device_copy(const MlpParams &p, float tau0)
 {
-    MlpDevice d{};
+    using lbm::kMlpK1;
+    using lbm::kMlpK2;
+    using lbm::kMlpN3;
+    using lbm::umma_index;
+    MlpDevice d{};  // zero: the padding columns and rows
     for (int n = 0; n < kMlpHidden; n++) {
         for (int k = 0; k < kMlpIn; k++)
-            d.w1[lbm::umma_index(n, k, kMlpHidden)] = __float2half_rn(p.w1[n * kMlpIn + k]);
+            d.w1[umma_index(n, k, kMlpHidden)] = __float2half_rn(p.w1[n * kMlpIn + k]);
+        d.w1[umma_index(n, kMlpIn, kMlpHidden)] = __float2half_rn(p.b1[n]);  // times the constant-1 column
         for (int k = 0; k < kMlpHidden; k++)
-            d.w2[lbm::umma_index(n, k, kMlpHidden)] = __float2half_rn(p.w2[n * kMlpHidden + k]);
+            d.w2[umma_index(n, k, kMlpHidden)] = __float2half_rn(p.w2[n * kMlpHidden + k]);
+        d.w2[umma_index(n, kMlpHidden, kMlpHidden)] = __float2half_rn(p.b2[n]);
+        d.w3[umma_index(0, n, kMlpN3)] = __float2half_rn(p.w3[n]);
     }
-    std::memcpy(d.b1, p.b1, sizeof(d.b1));
-    std::memcpy(d.b2, p.b2, sizeof(d.b2));
-    std::memcpy(d.w3, p.w3, sizeof(d.w3));
-    d.b3 = p.b3;
+    d.w3[umma_index(0, kMlpHidden, kMlpN3)] = __float2half_rn(p.b3);
+    static_assert(kMlpK1 > kMlpIn && kMlpK2 > kMlpHidden, "room for the constant column");
     std::memcpy(d.in_scale, p.in_scale, sizeof(d.in_scale));
     for (int k = 0; k < kMlpIn; k++)
         d.in_shift[k] = -p.in_mean[k] * p.in_scale[k];
@@ -408,12 +414,32 @@ lbm_status launch_infer(const float *src, size_t N, const MlpDevice &net, float 
     void *fn = from_moments ? (raw_y ? (void *)&lbm::mlp_infer_kernel<true, true> : (void *)&lbm::mlp_infer_kernel<true, false>)
                             : (raw_y ? (void *)&lbm::mlp_infer_kernel<false, true> : (void *)&lbm::mlp_infer_kernel<false, false>);
     static_assert(lbm::MlpSmem::BYTES <= lbm::MlpSmem::LAUNCH_BYTES, "layout");
-    LBM_CUDA_RETURN(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, lbm::MlpSmem::LAUNCH_BYTES));
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    // the shared-memory attribute and the SM count, once per kernel and
+    // device (these calls are far slower than a launch)
+    struct Known {
+        const void *fn;
+        int device, sms;
+    };
+    static std::mutex mu;
+    static std::vector<Known> known;
+    int sms = 0;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        for (const Known &k : known)
+            if (k.fn == fn && k.device == device)
+                sms = k.sms;
+        if (sms == 0) {
+            LBM_CUDA_RETURN(
+                cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, lbm::MlpSmem::LAUNCH_BYTES));
+            LBM_CUDA_RETURN(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+            known.push_back({fn, device, sms});
+        }
+    }
     const size_t tiles = (N + 127) / 128;
-    // 8 CTAs per SM: the register limit at 64 per thread (8 x 32 tensor-memory columns fit)
-    const unsigned grid = unsigned(std::min<size_t>(tiles, size_t(sms) * 8));
+    // persistent: one wave of the CTAs the register budget keeps resident
+    // (at most 8 per SM by shared memory, so their 32 tensor-memory columns
+    // each fit the SM's 512)
+    const unsigned grid = unsigned(std::min<size_t>(tiles, size_t(sms) * lbm::kMlpCtasPerSm));
     uint64_t timeout = 2000000000ull;
     MlpDevice net_arg = net;
     void *args[] = {&src, &N, &net_arg, &out, &err, &timeout};

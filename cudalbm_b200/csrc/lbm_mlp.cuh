@@ -12,16 +12,19 @@
 //
 // Two evaluations:
 //   * mlp_forward_f32: FP32 on CUDA cores (training, reference path);
-//   * mlp_infer_kernel: tensor cores.  A CTA of 128 threads takes 128 nodes
-//     (one per thread = one row of M = 128): each thread writes its features
-//     in FP16 into shared memory in the UMMA canonical K-major layout, one
-//     thread issues tcgen05.mma (kind::f16, FP32 accumulators in tensor
-//     memory) for 16 -> 32, every warp reads its 32 rows back with
-//     tcgen05.ld, applies bias + GELU, writes FP16 activations for 32 -> 32
-//     (two K = 16 MMAs into the same 32 tensor-memory columns), reads back,
-//     and finishes the 32 -> 1 layer on CUDA cores; the next tile's node
-//     values are loaded meanwhile.  Weights are FP16 (converted once on the host into the operand
-//     layout), accumulation FP32.
+//   * mlp_infer_kernel: tensor cores for all three layers.  A CTA of 128
+//     threads takes 128 nodes (one per thread = one row of M = 128): each
+//     thread writes its standardised features in FP16 into shared memory in
+//     the UMMA canonical K-major layout, one thread issues tcgen05.mma
+//     (kind::f16, FP32 accumulators in tensor memory), every warp reads its
+//     32 rows back with tcgen05.ld, applies GELU in packed FP16 (two values
+//     per instruction, tanh.approx.f16x2) and writes the FP16 activations as
+//     the next layer's operand; the 32 -> 1 layer is an N = 16 MMA whose
+//     first column is y.  Every operand carries a constant-1 column after its
+//     values (K = 16 + 1 -> 32, 32 + 1 -> 48), so the weight operands hold
+//     the biases and the tensor cores add them.  Weights and biases are FP16
+//     (converted once on the host into the operand layout), accumulation
+//     FP32; the next tile's node values are loaded meanwhile.
 #pragma once
 
 #include <cuda_fp16.h>
@@ -46,12 +49,18 @@ struct MlpParams {
 };
 constexpr int kMlpWeights = kMlpHidden * kMlpIn + kMlpHidden + kMlpHidden * kMlpHidden + kMlpHidden + kMlpHidden + 1;
 
-// Device copy for the tensor-core path: FP16 weights already in the operand
-// layout (umma_index), FP32 vectors.
+// Operand widths of the tensor-core path: K of the layer-1 operand (16
+// features, the constant 1, zeros), K of the hidden-activation operand (32
+// values, the constant 1, zeros), N of the output layer (y in column 0).
+constexpr int kMlpK1 = 32, kMlpK2 = 48, kMlpN3 = 16;
+
+// Device copy for the tensor-core path: FP16 weight operands already in the
+// operand layout (umma_index), bias in the column of the constant-1 input;
+// FP32 feature normalisation and output clamp.
 struct MlpDevice {
-    __half w1[kMlpHidden * kMlpIn];
-    __half w2[kMlpHidden * kMlpHidden];
-    float b1[kMlpHidden], b2[kMlpHidden], w3[kMlpHidden], b3;
+    __half w1[kMlpHidden * kMlpK1];  // [32 out][w1 | b1 | 0]
+    __half w2[kMlpHidden * kMlpK2];  // [32 out][w2 | b2 | 0]
+    __half w3[kMlpN3 * kMlpK2];      // row 0: [w3 | b3 | 0], rows 1-15 zero
     float in_scale[kMlpIn], in_shift[kMlpIn], in_lo[kMlpIn], in_hi[kMlpIn];  // x = f * scale + shift
     float out_scale, dtau_lo, dtau_hi;
     float r_ii, r_ij;  // 1 / (2 * 4.5 * tau0), 1 / (2 * 9 * tau0) for the strain-rate features
@@ -73,29 +82,37 @@ __device__ __forceinline__ float gelu(float x)
 {
     return 0.5f * x * (1.0f + tanhf(kGeluA * fmaf(kGeluB * x * x, x, x)));
 }
-// hardware tanh (tanh.approx.f32; its error is below the FP16 rounding of
-// the activations that follow) for the tensor-core path
-__device__ __forceinline__ float gelu_fast(float x)
+// Two FP32 values as FP16x2 (lo in the low half), rounded to nearest and
+// saturated to the largest finite FP16 (so no infinity reaches the GELU).
+__device__ __forceinline__ uint32_t pack_f16x2_sat(float lo, float hi)
 {
-    float t;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(kGeluA * fmaf(kGeluB * x * x, x, x)));
-    return 0.5f * x * (1.0f + t);
+    uint32_t d;
+    asm("cvt.rn.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+    return d;
 }
 
-// One row (one node) of an FP16 operand in umma_index layout: K values, stored
-// as K/8 16-byte vectors (consecutive rows are consecutive 16-byte slots of a
-// core matrix, so a warp's stores do not conflict).
-template <int K>
-__device__ __forceinline__ void store_row_f16(__half *base, int row, const float *v)
+// GELU of two FP16 values in packed FP16 arithmetic: x^2, a (1 + b x^2),
+// x a (1 + b x^2), tanh.approx.f16x2, then 0.5 x + 0.5 x tanh.  Finite inputs
+// give finite outputs (tanh saturates to +-1).
+__device__ __forceinline__ uint32_t gelu_f16x2(uint32_t xu)
 {
-#pragma unroll
-    for (int c = 0; c < K / 8; c++) {
-        __align__(16) __half2 h[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-            h[j] = __floats2half2_rn(v[8 * c + 2 * j], v[8 * c + 2 * j + 1]);
-        *reinterpret_cast<uint4 *>(base + umma_index(row, 8 * c, 128)) = *reinterpret_cast<const uint4 *>(h);
-    }
+    const __half2 x = *reinterpret_cast<const __half2 *>(&xu);
+    const __half2 a = __float2half2_rn(kGeluA), ab = __float2half2_rn(kGeluA * kGeluB);
+    const __half2 u = __hmul2(x, __hfma2(__hmul2(x, x), ab, a));
+    uint32_t t;
+    asm("tanh.approx.f16x2 %0, %1;" : "=r"(t) : "r"(*reinterpret_cast<const uint32_t *>(&u)));
+    const __half2 hx = __hmul2(x, __float2half2_rn(0.5f));
+    const __half2 g = __hfma2(hx, *reinterpret_cast<const __half2 *>(&t), hx);
+    return *reinterpret_cast<const uint32_t *>(&g);
+}
+
+// 8 consecutive K values (4 packed pairs) of one row of an FP16 operand in
+// umma_index layout with `rows` rows: one 16-byte store (consecutive rows are
+// consecutive 16-byte slots of a core matrix, so a warp's stores do not conflict).
+__device__ __forceinline__ void store_chunk_f16(__half *base, int row, int k0, int rows, uint32_t p0, uint32_t p1,
+                                                uint32_t p2, uint32_t p3)
+{
+    *reinterpret_cast<uint4 *>(base + umma_index(row, k0, rows)) = make_uint4(p0, p1, p2, p3);
 }
 
 // The 16 raw features of a node from its 10 stored moments (rho - 1, 3u, ...).
@@ -220,6 +237,15 @@ __device__ __forceinline__ void tmem_dealloc_warp(uint32_t taddr, uint32_t ncols
 {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
 }
+// One FP32 column of this thread's tensor-memory lane.
+__device__ __forceinline__ float tmem_ld_1col(uint32_t taddr)
+{
+    __syncwarp();  // .sync.aligned: the lanes may leave a bounded wait at different times
+    uint32_t r;
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr) : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    return __uint_as_float(r);
+}
 // 32 consecutive FP32 columns of this thread's tensor-memory lane.
 __device__ __forceinline__ void tmem_ld_32cols(uint32_t taddr, float *v)
 {
@@ -243,67 +269,130 @@ __device__ __forceinline__ void tmem_ld_32cols(uint32_t taddr, float *v)
 // ------------------------------------------------------- inference kernel
 // Shared memory of mlp_infer_kernel (byte offsets; operands 128 B aligned).
 struct MlpSmem {
-    static constexpr int W1 = 0;                          // 32 x 16 FP16, 1 KB
-    static constexpr int W2 = W1 + kMlpHidden * kMlpIn * 2;   // 32 x 32 FP16, 2 KB
-    static constexpr int A1 = W2 + kMlpHidden * kMlpHidden * 2;  // 128 x 16 FP16, 4 KB
-    static constexpr int A2 = A1 + 128 * kMlpIn * 2;          // 128 x 32 FP16, 8 KB
-    static constexpr int BAR = A2 + 128 * kMlpHidden * 2;     // mbarrier
-    static constexpr int TMEM = BAR + 8;                      // allocated tensor-memory address
-    static constexpr int FLAG = TMEM + 4;                     // abort flag
-    static constexpr int BYTES = FLAG + 4;
-    // shared memory requested per CTA: with at most 14 CTAs on an SM (227 KB),
-    // their 14 x 32 tensor-memory columns never exceed the SM's 512
-    static constexpr int LAUNCH_BYTES = 16 * 1024;
-    // leading (K-chunk) byte offsets of the operands; the stride between
-    // 8-row groups is 128 B for all of them
-    static constexpr uint32_t LBO_W = (kMlpHidden / 8) * 128, LBO_A = (128 / 8) * 128, SBO = 128;
+    static constexpr int W1 = 0;                                  // 32 x 32 FP16, 2 KB
+    static constexpr int W2 = W1 + kMlpHidden * kMlpK1 * 2;       // 32 x 48 FP16, 3 KB
+    static constexpr int W3 = W2 + kMlpHidden * kMlpK2 * 2;       // 16 x 48 FP16, 1.5 KB
+    static constexpr int A1 = W3 + kMlpN3 * kMlpK2 * 2;           // 128 x 32 FP16, 8 KB (features)
+    static constexpr int A2 = A1 + 128 * kMlpK1 * 2;              // 128 x 48 FP16, 12 KB (activations)
+    static constexpr int BAR = A2 + 128 * kMlpK2 * 2;             // mbarrier
+    static constexpr int TMEM = BAR + 8;                          // allocated tensor-memory address
+    static constexpr int BYTES = TMEM + 4;
+    // shared memory requested per CTA: at most 8 CTAs on an SM (228 KB, 1 KB
+    // reserved each), so their 8 x 32 tensor-memory columns fit the SM's 512
+    static constexpr int LAUNCH_BYTES = 27 * 1024;
+    // leading (K-chunk) byte offsets: (rows / 8) x 128 B; the stride between
+    // 8-row groups is 128 B for all operands
+    static constexpr uint32_t LBO_W = (kMlpHidden / 8) * 128, LBO_W3 = (kMlpN3 / 8) * 128, LBO_A = (128 / 8) * 128,
+                              SBO = 128;
 };
+static_assert(MlpSmem::A1 % 128 == 0 && MlpSmem::A2 % 128 == 0 && MlpSmem::W3 % 128 == 0, "operand alignment");
 
 enum : unsigned { ERR_MMA_TIMEOUT = 2u };
 
-// The network is a kernel parameter (constant bank: its uniform values feed
-// instructions directly).  Source of a node's 16 raw features: stored moments [10][N] (FROM_MOMENTS)
-// or a feature array [N][16].  Output dtau[N] (clamped, 0 where the inputs
-// leave the training range), or the raw network output y[N] (RAW_Y).
+#ifndef LBM_MLP_CTAS_PER_SM
+#define LBM_MLP_CTAS_PER_SM 8
+#endif
+// CTAs per SM the register budget is sized for (the launch's grid is one wave of them)
+constexpr int kMlpCtasPerSm = LBM_MLP_CTAS_PER_SM;
+static_assert(kMlpCtasPerSm * 32 <= 512 && kMlpCtasPerSm * (MlpSmem::LAUNCH_BYTES + 1024) <= 228 * 1024,
+              "tensor-memory columns and shared memory of the resident CTAs");
+
+// The network is a kernel parameter (constant bank).  Source of a node's 16
+// raw features: stored moments [10][N] (FROM_MOMENTS) or a feature array
+// [N][16].  Output dtau[N] (clamped, 0 where the inputs leave the training
+// range), or the raw network output y[N] (RAW_Y).
 template <bool FROM_MOMENTS, bool RAW_Y>
-__global__ void __launch_bounds__(128, 8) mlp_infer_kernel(const float *src, size_t N,
+__global__ void __launch_bounds__(128, kMlpCtasPerSm) mlp_infer_kernel(const float *src, size_t N,
                                                            const __grid_constant__ MlpDevice net, float *out,
                                                            unsigned *err, uint64_t timeout_ns)
 {
     extern __shared__ __align__(1024) unsigned char sm[];
     __half *w1 = reinterpret_cast<__half *>(sm + MlpSmem::W1);
     __half *w2 = reinterpret_cast<__half *>(sm + MlpSmem::W2);
+    __half *w3 = reinterpret_cast<__half *>(sm + MlpSmem::W3);
     __half *a1 = reinterpret_cast<__half *>(sm + MlpSmem::A1);
     __half *a2 = reinterpret_cast<__half *>(sm + MlpSmem::A2);
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + MlpSmem::BAR);
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(sm + MlpSmem::TMEM);
-    int *flag = reinterpret_cast<int *>(sm + MlpSmem::FLAG);
     const int tid = threadIdx.x, warp = tid >> 5;
     const bool leader = tid == 0;
 
-    // weights (already in operand layout) into shared memory
-    for (int i = tid; i < kMlpHidden * kMlpIn; i += 128)
-        w1[i] = net.w1[i];
-    for (int i = tid; i < kMlpHidden * kMlpHidden; i += 128)
-        w2[i] = net.w2[i];
+    // weights (already in operand layout) into shared memory, 4 B at a time
+    // (the parameter block guarantees 4-byte alignment)
+    {
+        const uint32_t *g = reinterpret_cast<const uint32_t *>(net.w1);
+        uint32_t *d = reinterpret_cast<uint32_t *>(sm + MlpSmem::W1);
+        constexpr int n4 = (MlpSmem::A1 - MlpSmem::W1) / 4;  // w1, w2, w3 are contiguous in both
+        static_assert(sizeof(net.w1) + sizeof(net.w2) + sizeof(net.w3) == MlpSmem::A1 - MlpSmem::W1, "weights");
+        for (int i = tid; i < n4; i += 128)
+            d[i] = g[i];
+    }
+    // the constant columns of this thread's operand rows: 1 after the values, then zeros
+    const uint32_t one_lo = 0x3C00u;  // FP16 1.0 in the low half
+    store_chunk_f16(a1, tid, kMlpIn, 128, one_lo, 0u, 0u, 0u);
+    store_chunk_f16(a1, tid, kMlpIn + 8, 128, 0u, 0u, 0u, 0u);
+    store_chunk_f16(a2, tid, kMlpHidden, 128, one_lo, 0u, 0u, 0u);
+    store_chunk_f16(a2, tid, kMlpHidden + 8, 128, 0u, 0u, 0u, 0u);
     mbar_init_if(leader, bar);
     fence_mbar_init_if(leader);
-    *flag = 0;
     __syncwarp();
     if (warp == 0)
-        tmem_alloc_warp(tmem_slot, 32);  // 32 FP32 columns: layer 1, then layer 2
+        tmem_alloc_warp(tmem_slot, 32);  // 32 FP32 columns, reused by the three layers
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     cta_sync();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
     const uint32_t lane_base = uint32_t(warp * 32) << 16;
-    constexpr uint32_t idesc = umma_idesc_f16_f32<128, kMlpHidden>();
-    const uint64_t d_w1 = umma_desc(w1, MlpSmem::LBO_W, MlpSmem::SBO);
-    const uint64_t d_a1 = umma_desc(a1, MlpSmem::LBO_A, MlpSmem::SBO);
+    constexpr uint32_t idesc_h = umma_idesc_f16_f32<128, kMlpHidden>();
+    constexpr uint32_t idesc_o = umma_idesc_f16_f32<128, kMlpN3>();
     unsigned phase = 0;
+    bool failed = false;   // warp 0's MMA wait gave up
+    bool aborted = false;  // uniform: from the barrier's OR-reduction
+    // One layer: a barrier (the operand is written, the previous
+    // accumulators are read), the K-steps (16 each) and their commit issued by
+    // one thread, the completion awaited by warp 0 alone (bounded) while the
+    // other warps sleep in the second barrier, whose OR-reduction tells every
+    // thread whether the wait gave up (false: stop).
+    auto layer = [&](const __half *a, const __half *w, uint32_t lbo_w, int ksteps, uint32_t idesc) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        cta_sync();
+        tc_fence_after();
+        for (int s = 0; s < ksteps; s++)
+            umma_f16_if(leader, tmem, umma_desc(a + s * MlpSmem::LBO_A, MlpSmem::LBO_A, MlpSmem::SBO),
+                        umma_desc(w + s * lbo_w, lbo_w, MlpSmem::SBO), idesc, s > 0);
+        umma_commit_if(leader, bar);
+        if (warp == 0 && !mbar_wait_bounded(bar, phase, timeout_ns)) {
+            if (leader)
+                atomicOr(err, ERR_MMA_TIMEOUT);
+            failed = true;
+        }
+        phase ^= 1u;
+        __syncwarp();
+        if (__syncthreads_or(failed)) {
+            aborted = true;
+            return false;
+        }
+        tc_fence_after();
+        return true;
+    };
+    // accumulators (bias included) -> GELU in FP16 -> the activation operand
+    auto activate = [&]() {
+        float z[kMlpHidden];
+        tmem_ld_32cols(tmem + lane_base, z);
+#pragma unroll
+        for (int c = 0; c < kMlpHidden / 8; c++) {
+            uint32_t p[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                p[j] = gelu_f16x2(pack_f16x2_sat(z[8 * c + 2 * j], z[8 * c + 2 * j + 1]));
+            store_chunk_f16(a2, tid, 8 * c, 128, p[0], p[1], p[2], p[3]);
+        }
+    };
 
     const size_t tiles = (N + 127) / 128;
+    constexpr int NV = FROM_MOMENTS ? 10 : kMlpIn;  // values loaded per node
     // node values of the next tile are loaded while the current one computes
     auto load = [&](size_t tile, float *v) {
         const size_t node = tile * 128 + tid;
@@ -319,12 +408,11 @@ __global__ void __launch_bounds__(128, 8) mlp_infer_kernel(const float *src, siz
             }
         } else {
 #pragma unroll
-            for (int k = 0; k < kMlpIn; k++)
+            for (int k = 0; k < NV; k++)
                 v[k] = 0.0f;
         }
     };
-    constexpr int NV = FROM_MOMENTS ? 10 : kMlpIn;
-    float next[kMlpIn];
+    float next[NV];
     load(blockIdx.x, next);
     for (size_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const size_t node = tile * 128 + tid;
@@ -337,69 +425,39 @@ __global__ void __launch_bounds__(128, 8) mlp_infer_kernel(const float *src, siz
             for (int k = 0; k < kMlpIn; k++)
                 f[k] = next[k];
         }
-        (void)NV;
         load(tile + gridDim.x, next);
         const bool inside = valid && in_range(f, net);
-        // layer 1 operand: this thread's row of standardised features
+        // layer-1 operand: this thread's row of standardised features
 #pragma unroll
-        for (int k = 0; k < kMlpIn; k++)
-            f[k] = fmaf(f[k], net.in_scale[k], net.in_shift[k]);
-        store_row_f16<kMlpIn>(a1, tid, f);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        tc_fence_before();
-        cta_sync();
-        tc_fence_after();
-        umma_f16_if(leader, tmem, d_a1, d_w1, idesc, false);
-        umma_commit_if(leader, bar);
-        if (!mbar_wait_bounded(bar, phase, timeout_ns)) {
-            atomicOr(err, ERR_MMA_TIMEOUT);
-            *flag = 1;
+        for (int c = 0; c < kMlpIn / 8; c++) {
+            uint32_t p[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                p[j] = pack_f16x2_sat(fmaf(f[8 * c + 2 * j], net.in_scale[8 * c + 2 * j], net.in_shift[8 * c + 2 * j]),
+                                      fmaf(f[8 * c + 2 * j + 1], net.in_scale[8 * c + 2 * j + 1],
+                                           net.in_shift[8 * c + 2 * j + 1]));
+            store_chunk_f16(a1, tid, 8 * c, 128, p[0], p[1], p[2], p[3]);
         }
-        phase ^= 1u;
-        tc_fence_after();
-        float h[kMlpHidden];
-        tmem_ld_32cols(tmem + lane_base, h);
-#pragma unroll
-        for (int j = 0; j < kMlpHidden; j++)
-            h[j] = gelu_fast(h[j] + net.b1[j]);
-        store_row_f16<kMlpHidden>(a2, tid, h);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        // every thread has read its layer-1 accumulators (tcgen05.wait::ld):
-        // layer 2 may overwrite the same columns
-        tc_fence_before();
-        cta_sync();
-        if (*flag)
+        // each layer starts at a barrier: the threads have read the previous
+        // layer's accumulators (tcgen05.wait::ld) and written its operand
+        if (!layer(a1, w1, MlpSmem::LBO_W, kMlpK1 / 16, idesc_h))  // 16 + 1 -> 32
             break;
-        tc_fence_after();
-        // layer 2: K = 32 as two K = 16 steps
-#pragma unroll
-        for (int s = 0; s < 2; s++)
-            umma_f16_if(leader, tmem, umma_desc(a2 + s * 2 * (MlpSmem::LBO_A / 2), MlpSmem::LBO_A, MlpSmem::SBO),
-                        umma_desc(w2 + s * 2 * (MlpSmem::LBO_W / 2), MlpSmem::LBO_W, MlpSmem::SBO), idesc, s > 0);
-        umma_commit_if(leader, bar);
-        if (!mbar_wait_bounded(bar, phase, timeout_ns)) {
-            atomicOr(err, ERR_MMA_TIMEOUT);
-            *flag = 1;
-        }
-        phase ^= 1u;
-        tc_fence_after();
-        tmem_ld_32cols(tmem + lane_base, h);
-        float y = net.b3;
-#pragma unroll
-        for (int j = 0; j < kMlpHidden; j++)
-            y = fmaf(net.w3[j], gelu_fast(h[j] + net.b2[j]), y);
+        activate();
+        if (!layer(a2, w2, MlpSmem::LBO_W, kMlpK2 / 16, idesc_h))  // 32 + 1 -> 32
+            break;
+        activate();
+        if (!layer(a2, w3, MlpSmem::LBO_W3, kMlpK2 / 16, idesc_o))  // 32 + 1 -> y
+            break;
+        const float y = tmem_ld_1col(tmem + lane_base);
         if (valid) {
             if constexpr (RAW_Y)
                 out[node] = y;
             else
                 out[node] = inside ? fminf(fmaxf(net.out_scale * y, net.dtau_lo), net.dtau_hi) : 0.0f;
         }
-        tc_fence_before();
-        cta_sync();
-        if (*flag)
-            break;
+        // the next tile's first barrier orders this read before its MMAs
     }
-    if (*flag) {
+    if (aborted) {
         // an MMA did not complete in time: give it a bounded chance to
         // finish before its tensor memory is released
         (void)mbar_wait_bounded(bar, phase ^ 1u, 1000000ull);

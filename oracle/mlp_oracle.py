@@ -51,21 +51,25 @@ def features(m, tau0):
     return np.concatenate([m, np.stack(s)], axis=0).T.astype(np.float32)
 
 
+def _h(a):
+    """Round to FP16 with saturation to the largest finite value."""
+    return np.clip(np.asarray(a, np.float64), -65504.0, 65504.0).astype(np.float16).astype(np.float64)
+
+
 def forward(p, feats, fp16=False):
-    """Network output y [n]; fp16=True rounds weights and the inputs of both
-    MMA layers to FP16 as the tensor-core path does (accumulation in FP64)."""
+    """Network output y [n]; fp16=True follows the tensor-core path's
+    roundings (accumulation in FP64): standardised inputs, weights and biases
+    in FP16, each layer's pre-activation rounded to FP16 before the GELU and
+    the activation rounded to FP16 after it.  (The device evaluates the GELU
+    in FP16 arithmetic, which this model rounds only once.)"""
     x = (np.asarray(feats, np.float64) - p["in_mean"]) * p["in_scale"]
-    w1, w2 = p["w1"], p["w2"]
-    if fp16:
-        x = x.astype(np.float16).astype(np.float64)
-        w1 = w1.astype(np.float16).astype(np.float64)
-        w2 = w2.astype(np.float16).astype(np.float64)
-    z1 = x @ w1.T + p["b1"]
-    h1 = gelu(z1)
-    if fp16:
-        h1 = h1.astype(np.float16).astype(np.float64)
-    z2 = h1 @ w2.T + p["b2"]
-    return gelu(z2) @ p["w3"] + p["b3"]
+    w1, w2, w3, b1, b2, b3 = p["w1"], p["w2"], p["w3"], p["b1"], p["b2"], p["b3"]
+    if not fp16:
+        h1 = gelu(x @ w1.T + b1)
+        return gelu(h1 @ w2.T + b2) @ w3 + b3
+    h1 = _h(gelu(_h(_h(x) @ _h(w1).T + _h(b1))))
+    h2 = _h(gelu(_h(h1 @ _h(w2).T + _h(b2))))
+    return h2 @ _h(w3) + _h(b3)
 
 
 def gradient(p, feats, targets):
