@@ -1,6 +1,6 @@
 """Learned-closure study: an under-resolved D3Q27 lid-driven cavity on a
-coarse grid, with and without the learned relaxation-time correction, judged
-by a fine run at twice the resolution.
+coarse grid, with and without the learned relaxation-time correction, measured
+against a fine run at twice the resolution.
 
     python -m cudalbm_b200.closure_study [--nc 128] [--coarse-steps 10000] [--seeds 8]
         [--snapshots 6] [--stride 3] [--json out.json]
@@ -18,10 +18,10 @@ Steps (all on the GPU through the library):
     one more perturbed fine run (seed ``seeds``, not used for training) --
     never against the evaluation case.
  4. Evaluation: the unperturbed case.  Plain coarse, learned coarse and the
-    fine run (the judge) advance the same physical time (coarse steps =
+    fine run (the truth) advance the same physical time (coarse steps =
     fine steps / 2 at equal lattice velocity).  Errors: centreline u(y) at
     x = z = mid and the whole velocity field, relative L2, against the fine
-    run box-filtered 2:1 (the stated judge) and against the fine run sampled
+    run box-filtered 2:1 (the stated measure) and against the fine run sampled
     at the coarse nodes' positions (trilinear; the 2:1 box filter places the
     coarse wall rows a quarter fine cell inside the walls).  Wall times of
     the coarse runs and of the fine run over the same physical time.
@@ -108,8 +108,8 @@ def run_study(nc: int = 128, lattice: int = 27, u_lid: float = 0.05, tau_coarse:
     cav = lambda n: Cavity(lattice, n, n, n, Re, u_lid, device=device)
     whole_field = nf <= field_pos_max
 
-    def fine_run(seed, trainer=None, judge_at=()):
-        """Fine run to Tf; samples at the snapshots, filtered states at judge_at."""
+    def fine_run(seed, trainer=None, truth_at=()):
+        """Fine run to Tf; samples at the snapshots, filtered states at truth_at."""
         out = {}
         with cav(nf) as f, cav(nc) as c:
             f.init_regions()
@@ -120,10 +120,10 @@ def run_study(nc: int = 128, lattice: int = 27, u_lid: float = 0.05, tau_coarse:
             f.synchronize()
             t0 = time.perf_counter()
             done = 0
-            for s in sorted(set(snaps if trainer is not None else []) | set(judge_at)):
+            for s in sorted(set(snaps if trainer is not None else []) | set(truth_at)):
                 f.step(s - done)
                 done = s
-                if s in judge_at:
+                if s in truth_at:
                     c.filter_from(f)
                     out[s // 2] = (c.read(), centreline_at_coarse_nodes(f, nc),
                                    sample_at_coarse_nodes(f.read()[1:4], nc) if whole_field else None)
@@ -137,7 +137,7 @@ def run_study(nc: int = 128, lattice: int = 27, u_lid: float = 0.05, tau_coarse:
             out["wall"] = time.perf_counter() - t0
         return out
 
-    def coarse_run(net, judge, times=(Tc // 2, Tc), dtau=False):
+    def coarse_run(net, truth, times=(Tc // 2, Tc), dtau=False):
         res = {}
         with cav(nc) as c:
             c.init_regions()
@@ -154,7 +154,7 @@ def run_study(nc: int = 128, lattice: int = 27, u_lid: float = 0.05, tau_coarse:
                 walls = time.perf_counter() - t0
                 done = t
                 m = c.read()
-                jb, jc, ji = judge[t]
+                jb, jc, ji = truth[t]
                 res[t] = {"centreline_box": rel(centreline(m), centreline(jb)),
                           "field_box": rel(m[1:4], jb[1:4]),
                           "centreline_pos": rel(centreline(m), jc),
@@ -186,7 +186,7 @@ def run_study(nc: int = 128, lattice: int = 27, u_lid: float = 0.05, tau_coarse:
     trainer.close()
 
     # calibration on a held-out perturbed seed
-    calib = fine_run(seeds, judge_at=(Tf,))
+    calib = fine_run(seeds, truth_at=(Tf,))
     base = net.out_scale
     scores = {}
     for a in shrink:
@@ -196,9 +196,9 @@ def run_study(nc: int = 128, lattice: int = 27, u_lid: float = 0.05, tau_coarse:
     net.out_scale = base * best
     log(f"calibration (centreline error on seed {seeds}): {scores} -> shrink {best}")
 
-    judge = fine_run(None, judge_at=(Tf // 2, Tf))
-    plain = coarse_run(None, judge)
-    learned = coarse_run(net, judge, dtau=True)
+    truth = fine_run(None, truth_at=(Tf // 2, Tf))
+    plain = coarse_run(None, truth)
+    learned = coarse_run(net, truth, dtau=True)
     if save:
         save_mlp(save, net)
     out = {
@@ -209,13 +209,13 @@ def run_study(nc: int = 128, lattice: int = 27, u_lid: float = 0.05, tau_coarse:
                      "loss_first": rep["loss_first"], "loss_last": rep["loss_last"], "r2_held_out": r2,
                      "shrink_scores": {str(k): v for k, v in scores.items()}, "shrink": best},
         "plain": plain, "learned": learned,
-        "fine_wall_s": judge["wall"],
-        "speedup_learned_vs_fine": judge["wall"] / learned["wall"],
+        "fine_wall_s": truth["wall"],
+        "speedup_learned_vs_fine": truth["wall"] / learned["wall"],
         "dtau": learned.pop("dtau"),
     }
     for t in (Tc // 2, Tc):
         log(f"t={t}: plain {plain[t]}  learned {learned[t]}")
-    log(f"wall: fine {judge['wall']:.2f} s, coarse plain {plain['wall']:.2f} s, coarse learned {learned['wall']:.2f} s")
+    log(f"wall: fine {truth['wall']:.2f} s, coarse plain {plain['wall']:.2f} s, coarse learned {learned['wall']:.2f} s")
     return out
 
 

@@ -2,7 +2,7 @@
 
 A reduced closure study (cudalbm_b200/closure_study.py): D3Q27 cavity on a
 32^3 grid at the coarse relaxation time 0.5077 (Re 604), trained on eight
-perturbed 64^3 runs, shrink factor calibrated on a ninth, judged by the
+perturbed 64^3 runs, shrink factor calibrated on a ninth, measured against the
 unperturbed 64^3 run box-filtered 2:1 (and sampled at the coarse nodes).
 Samples and training are deterministic, so the numbers below repeat.
 """

@@ -1,5 +1,5 @@
 """Self-check of the FP64 network oracle (CPU): its analytic gradient equals
-central finite differences, so it can judge the GPU training kernels."""
+central finite differences, so it can check the GPU training kernels."""
 import numpy as np
 
 from cudalbm_b200 import _lib
