@@ -351,6 +351,14 @@ dim3 grid_1d(size_t N)
     return dim3(unsigned(std::min<size_t>((N + 255) / 256, size_t(148) * 16)));
 }
 
+// Parameter blocks carry FP64 running means only for the kernels that keep
+// them: function objects on and mean_bits 64 (pick_fo); every other kernel
+// takes the FP32-mean block.
+bool means_f64(const lbm_handle *h)
+{
+    return h->cfg.function_objects != 0 && h->cfg.mean_bits == 64;
+}
+
 template <typename MeanT>
 lbm_status launch_step(lbm_handle *h, bool monitored = false)
 {
@@ -786,8 +794,9 @@ lbm_status ensure_steps_graph(lbm_handle *h)
     h->cur = 0;
     LBM_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     lbm_status s = LBM_OK;
+    const bool md = means_f64(h);
     for (uint64_t i = 0; i < kGraphSteps && s == LBM_OK; i++)
-        s = launch_step<float>(h);
+        s = md ? launch_step<double>(h) : launch_step<float>(h);
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     h->cur = cur0;
@@ -828,7 +837,7 @@ lbm_status lbm_step(lbm_handle *h, uint64_t n)
     LBM_CUDA(cudaSetDevice(h->cfg.device));
     if (n == 0)
         return LBM_OK;
-    const bool md = h->cfg.mean_bits == 64;
+    const bool md = means_f64(h);
     const bool graphed = !h->cfg.function_objects && !h->closure && n >= kGraphSteps;
     if (graphed) {
         // built once per kernel variant, outside the timed span
@@ -841,7 +850,7 @@ lbm_status lbm_step(lbm_handle *h, uint64_t n)
     if (graphed) {
         lbm_status s;
         if (h->cur != 0) {
-            if ((s = launch_step<float>(h)) != LBM_OK)
+            if ((s = md ? launch_step<double>(h) : launch_step<float>(h)) != LBM_OK)
                 return s;
             i++;
         }
@@ -870,7 +879,7 @@ lbm_status lbm_step_monitored(lbm_handle *h, uint64_t n, lbm_monitor *out)
     if (n == 0)
         return LBM_OK;
     LBM_CUDA(cudaEventRecord(h->ev0, h->stream));
-    const bool md = h->cfg.mean_bits == 64;
+    const bool md = means_f64(h);
     for (uint64_t i = 0; i < n; i++) {
         LBM_CUDA(cudaMemsetAsync(h->mon, 0, sizeof(lbm::MonitorSlot), h->stream));
         lbm_status s = md ? launch_step<double>(h, true) : launch_step<float>(h, true);
@@ -1225,7 +1234,7 @@ lbm_status lbm_autotune(lbm_handle *h, int32_t trial_steps, lbm_tuning *out)
         for (size_t i = 0; i < live.size(); i++)
             cudaMemcpyAsync(live[i].first, backup[i], live[i].second, cudaMemcpyDeviceToDevice, h->stream);
     };
-    const bool md = h->cfg.mean_bits == 64;
+    const bool md = means_f64(h);
     lbm_tuning best{};
     best.ms_per_step = 1e30;
     int tried = 0;

@@ -276,3 +276,20 @@ def test_graph_replay_equals_single_launches(q):
     assert bits_equal(a.read("moments"), b.read("moments"))
     a.close()
     b.close()
+
+
+def test_fp64_mean_setting_without_function_objects_is_the_plain_step():
+    """mean_bits = 64 matters only with function objects: without them the
+    step (graph-replayed or not) gives the FP32-mean handle's bits."""
+    a = Cavity(19, 32, 24, 16, 200.0, 0.05, mean_bits=64)
+    b = Cavity(19, 32, 24, 16, 200.0, 0.05)
+    for c in (a, b):
+        c.init_regions()
+    a.step(3)
+    a.step(37)
+    b.step(40)
+    a.synchronize()
+    b.synchronize()
+    assert bits_equal(a.read("moments"), b.read("moments"))
+    a.close()
+    b.close()
