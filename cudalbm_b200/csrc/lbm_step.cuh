@@ -195,6 +195,21 @@ struct StepParams {
     uint64_t timeout_ns;
     const float *dtau;  // per-node relaxation-time correction (closure kernels only)
 };
+// The host fills one block type for every storage format (the output is a
+// pointer), so the layouts must agree; FP32- and FP64-mean blocks differ only
+// inside the function-object fields.
+using StepParamsF32 = StepParams<float, float>;
+using StepParamsF16 = StepParams<float, __half>;
+using StepParamsBF16 = StepParams<float, __nv_bfloat16>;
+using StepParamsF64Means = StepParams<double, float>;
+static_assert(sizeof(StepParamsF32) == sizeof(StepParamsF16) && sizeof(StepParamsF32) == sizeof(StepParamsBF16) &&
+                  offsetof(StepParamsF32, dtau) == offsetof(StepParamsF16, dtau) &&
+                  offsetof(StepParamsF32, dtau) == offsetof(StepParamsBF16, dtau),
+              "parameter block layout must not depend on the storage type");
+static_assert(offsetof(StepParamsF32, fault) == offsetof(StepParamsF64Means, fault) &&
+                  offsetof(StepParamsF32, timeout_ns) == offsetof(StepParamsF64Means, timeout_ns) &&
+                  offsetof(StepParamsF32, dtau) == offsetof(StepParamsF64Means, dtau),
+              "fields after the function-object block at the same offsets for both mean precisions");
 
 template <int TX, int TY, typename ST = float>
 struct TileGeom {
