@@ -379,22 +379,17 @@ __global__ void forward_kernel(const float *feat, uint64_t n, const MlpParams *p
 // ------------------------------------------------------------- helpers
 MlpDevice device_copy(const MlpParams &p, float tau0)
 {
-    using lbm::kMlpK1;
-    using lbm::kMlpK2;
-    using lbm::kMlpN3;
-    using lbm::umma_index;
-    MlpDevice d{};  // zero: the padding columns and rows
+    MlpDevice d{};
     for (int n = 0; n < kMlpHidden; n++) {
         for (int k = 0; k < kMlpIn; k++)
-            d.w1[umma_index(n, k, kMlpHidden)] = __float2half_rn(p.w1[n * kMlpIn + k]);
-        d.w1[umma_index(n, kMlpIn, kMlpHidden)] = __float2half_rn(p.b1[n]);  // times the constant-1 column
+            d.w1[lbm::umma_index(n, k, kMlpHidden)] = __float2half_rn(p.w1[n * kMlpIn + k]);
         for (int k = 0; k < kMlpHidden; k++)
-            d.w2[umma_index(n, k, kMlpHidden)] = __float2half_rn(p.w2[n * kMlpHidden + k]);
-        d.w2[umma_index(n, kMlpHidden, kMlpHidden)] = __float2half_rn(p.b2[n]);
-        d.w3[umma_index(0, n, kMlpN3)] = __float2half_rn(p.w3[n]);
+            d.w2[lbm::umma_index(n, k, kMlpHidden)] = __float2half_rn(p.w2[n * kMlpHidden + k]);
     }
-    d.w3[umma_index(0, kMlpHidden, kMlpN3)] = __float2half_rn(p.b3);
-    static_assert(kMlpK1 > kMlpIn && kMlpK2 > kMlpHidden, "room for the constant column");
+    std::memcpy(d.b1, p.b1, sizeof(d.b1));
+    std::memcpy(d.b2, p.b2, sizeof(d.b2));
+    std::memcpy(d.w3, p.w3, sizeof(d.w3));
+    d.b3 = p.b3;
     std::memcpy(d.in_scale, p.in_scale, sizeof(d.in_scale));
     for (int k = 0; k < kMlpIn; k++)
         d.in_shift[k] = -p.in_mean[k] * p.in_scale[k];

@@ -12,19 +12,20 @@
 //
 // Two evaluations:
 //   * mlp_forward_f32: FP32 on CUDA cores (training, reference path);
-//   * mlp_infer_kernel: tensor cores for all three layers.  A CTA of 128
-//     threads takes 128 nodes (one per thread = one row of M = 128): each
+//   * mlp_infer_kernel: the two hidden layers on the tensor cores.  A CTA of
+//     128 threads takes 128 nodes (one per thread = one row of M = 128): each
 //     thread writes its standardised features in FP16 into shared memory in
 //     the UMMA canonical K-major layout, one thread issues tcgen05.mma
 //     (kind::f16, FP32 accumulators in tensor memory), every warp reads its
-//     32 rows back with tcgen05.ld, applies GELU in packed FP16 (two values
-//     per instruction, tanh.approx.f16x2) and writes the FP16 activations as
-//     the next layer's operand; the 32 -> 1 layer is an N = 16 MMA whose
-//     first column is y.  Every operand carries a constant-1 column after its
-//     values (K = 16 + 1 -> 32, 32 + 1 -> 48), so the weight operands hold
-//     the biases and the tensor cores add them.  Weights and biases are FP16
-//     (converted once on the host into the operand layout), accumulation
-//     FP32; the next tile's node values are loaded meanwhile.
+//     32 rows back with tcgen05.ld, adds the biases in FP32, applies GELU in
+//     packed FP16 (two values per instruction, tanh.approx.f16x2) and writes
+//     the FP16 activations as the layer-2 operand; the 32 -> 1 layer runs on
+//     CUDA cores in FP32 from the FP16 activations.  An MMA costs the tensor
+//     pipe about the same time for any N up to 128 (measured: ~126 cycles
+//     per M = 128, K = 16 instruction, back to back), so the kernel issues the
+//     fewest: one for layer 1 (K = 16), two for layer 2 (K = 32).  Weights are
+//     FP16 (converted once on the host into the operand layout), biases and
+//     accumulation FP32; the next tile's node values are loaded meanwhile.
 #pragma once
 
 #include <cuda_fp16.h>
@@ -49,18 +50,12 @@ struct MlpParams {
 };
 constexpr int kMlpWeights = kMlpHidden * kMlpIn + kMlpHidden + kMlpHidden * kMlpHidden + kMlpHidden + kMlpHidden + 1;
 
-// Operand widths of the tensor-core path: K of the layer-1 operand (16
-// features, the constant 1, zeros), K of the hidden-activation operand (32
-// values, the constant 1, zeros), N of the output layer (y in column 0).
-constexpr int kMlpK1 = 32, kMlpK2 = 48, kMlpN3 = 16;
-
-// Device copy for the tensor-core path: FP16 weight operands already in the
-// operand layout (umma_index), bias in the column of the constant-1 input;
-// FP32 feature normalisation and output clamp.
+// Device copy for the tensor-core path: FP16 weights already in the operand
+// layout (umma_index), FP32 vectors.
 struct MlpDevice {
-    __half w1[kMlpHidden * kMlpK1];  // [32 out][w1 | b1 | 0]
-    __half w2[kMlpHidden * kMlpK2];  // [32 out][w2 | b2 | 0]
-    __half w3[kMlpN3 * kMlpK2];      // row 0: [w3 | b3 | 0], rows 1-15 zero
+    __half w1[kMlpHidden * kMlpIn];      // [32 out][16 in]
+    __half w2[kMlpHidden * kMlpHidden];  // [32 out][32 in]
+    float b1[kMlpHidden], b2[kMlpHidden], w3[kMlpHidden], b3;
     float in_scale[kMlpIn], in_shift[kMlpIn], in_lo[kMlpIn], in_hi[kMlpIn];  // x = f * scale + shift
     float out_scale, dtau_lo, dtau_hi;
     float r_ii, r_ij;  // 1 / (2 * 4.5 * tau0), 1 / (2 * 9 * tau0) for the strain-rate features
@@ -237,15 +232,6 @@ __device__ __forceinline__ void tmem_dealloc_warp(uint32_t taddr, uint32_t ncols
 {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
 }
-// One FP32 column of this thread's tensor-memory lane.
-__device__ __forceinline__ float tmem_ld_1col(uint32_t taddr)
-{
-    __syncwarp();  // .sync.aligned: the lanes may leave a bounded wait at different times
-    uint32_t r;
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr) : "memory");
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    return __uint_as_float(r);
-}
 // 32 consecutive FP32 columns of this thread's tensor-memory lane.
 __device__ __forceinline__ void tmem_ld_32cols(uint32_t taddr, float *v)
 {
@@ -266,26 +252,55 @@ __device__ __forceinline__ void tmem_ld_32cols(uint32_t taddr, float *v)
         v[j] = __uint_as_float(r[j]);
 }
 
+// Bounded mbarrier wait that sleeps in the barrier unit between checks
+// (try_wait with a suspend-time hint, in ns) instead of spinning on it, so a
+// waiting warp takes no issue slots from the warps that compute.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t *bar, unsigned parity, uint32_t hint_ns)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_sleep_bounded(uint64_t *bar, unsigned parity, uint64_t limit_ns)
+{
+    if (mbar_try_wait_sleep(bar, parity, 1000u))
+        return true;
+    const uint64_t t0 = global_ns();
+    for (;;) {
+        if (mbar_try_wait_sleep(bar, parity, 1000u))
+            return true;
+        if (global_ns() - t0 > limit_ns)
+            return false;
+    }
+}
+
 // ------------------------------------------------------- inference kernel
 // Shared memory of mlp_infer_kernel (byte offsets; operands 128 B aligned).
 struct MlpSmem {
-    static constexpr int W1 = 0;                                  // 32 x 32 FP16, 2 KB
-    static constexpr int W2 = W1 + kMlpHidden * kMlpK1 * 2;       // 32 x 48 FP16, 3 KB
-    static constexpr int W3 = W2 + kMlpHidden * kMlpK2 * 2;       // 16 x 48 FP16, 1.5 KB
-    static constexpr int A1 = W3 + kMlpN3 * kMlpK2 * 2;           // 128 x 32 FP16, 8 KB (features)
-    static constexpr int A2 = A1 + 128 * kMlpK1 * 2;              // 128 x 48 FP16, 12 KB (activations)
-    static constexpr int BAR = A2 + 128 * kMlpK2 * 2;             // mbarrier
-    static constexpr int TMEM = BAR + 8;                          // allocated tensor-memory address
+    static constexpr int W1 = 0;                                 // 32 x 16 FP16, 1 KB
+    static constexpr int W2 = W1 + kMlpHidden * kMlpIn * 2;      // 32 x 32 FP16, 2 KB
+    static constexpr int A1 = W2 + kMlpHidden * kMlpHidden * 2;  // 128 x 16 FP16, 4 KB (features)
+    static constexpr int A2 = A1 + 128 * kMlpIn * 2;             // 128 x 32 FP16, 8 KB (layer-1 activations)
+    static constexpr int BAR = A2 + 128 * kMlpHidden * 2;        // mbarrier
+    static constexpr int TMEM = BAR + 8;                         // allocated tensor-memory address
     static constexpr int BYTES = TMEM + 4;
-    // shared memory requested per CTA: at most 8 CTAs on an SM (228 KB, 1 KB
-    // reserved each), so their 8 x 32 tensor-memory columns fit the SM's 512
-    static constexpr int LAUNCH_BYTES = 27 * 1024;
+    // shared memory requested per CTA: at most 13 CTAs fit an SM (228 KB,
+    // 1 KB reserved each), and 13 x 32 tensor-memory columns fit its 512
+    static constexpr int LAUNCH_BYTES = 16 * 1024;
     // leading (K-chunk) byte offsets: (rows / 8) x 128 B; the stride between
     // 8-row groups is 128 B for all operands
-    static constexpr uint32_t LBO_W = (kMlpHidden / 8) * 128, LBO_W3 = (kMlpN3 / 8) * 128, LBO_A = (128 / 8) * 128,
-                              SBO = 128;
+    static constexpr uint32_t LBO_W = (kMlpHidden / 8) * 128, LBO_A = (128 / 8) * 128, SBO = 128;
 };
-static_assert(MlpSmem::A1 % 128 == 0 && MlpSmem::A2 % 128 == 0 && MlpSmem::W3 % 128 == 0, "operand alignment");
+static_assert(MlpSmem::A1 % 128 == 0 && MlpSmem::A2 % 128 == 0 && MlpSmem::W2 % 128 == 0, "operand alignment");
+static_assert(MlpSmem::BYTES <= MlpSmem::LAUNCH_BYTES &&
+                  (228 * 1024 / (MlpSmem::LAUNCH_BYTES + 1024)) * 32 <= 512,
+              "the CTAs shared memory admits to an SM must fit its tensor memory");
 
 enum : unsigned { ERR_MMA_TIMEOUT = 2u };
 
@@ -294,8 +309,6 @@ enum : unsigned { ERR_MMA_TIMEOUT = 2u };
 #endif
 // CTAs per SM the register budget is sized for (the launch's grid is one wave of them)
 constexpr int kMlpCtasPerSm = LBM_MLP_CTAS_PER_SM;
-static_assert(kMlpCtasPerSm * 32 <= 512 && kMlpCtasPerSm * (MlpSmem::LAUNCH_BYTES + 1024) <= 228 * 1024,
-              "tensor-memory columns and shared memory of the resident CTAs");
 
 // The network is a kernel parameter (constant bank).  Source of a node's 16
 // raw features: stored moments [10][N] (FROM_MOMENTS) or a feature array
@@ -303,13 +316,12 @@ static_assert(kMlpCtasPerSm * 32 <= 512 && kMlpCtasPerSm * (MlpSmem::LAUNCH_BYTE
 // range), or the raw network output y[N] (RAW_Y).
 template <bool FROM_MOMENTS, bool RAW_Y>
 __global__ void __launch_bounds__(128, kMlpCtasPerSm) mlp_infer_kernel(const float *src, size_t N,
-                                                           const __grid_constant__ MlpDevice net, float *out,
-                                                           unsigned *err, uint64_t timeout_ns)
+                                                                       const __grid_constant__ MlpDevice net,
+                                                                       float *out, unsigned *err, uint64_t timeout_ns)
 {
     extern __shared__ __align__(1024) unsigned char sm[];
     __half *w1 = reinterpret_cast<__half *>(sm + MlpSmem::W1);
     __half *w2 = reinterpret_cast<__half *>(sm + MlpSmem::W2);
-    __half *w3 = reinterpret_cast<__half *>(sm + MlpSmem::W3);
     __half *a1 = reinterpret_cast<__half *>(sm + MlpSmem::A1);
     __half *a2 = reinterpret_cast<__half *>(sm + MlpSmem::A2);
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + MlpSmem::BAR);
@@ -322,48 +334,41 @@ __global__ void __launch_bounds__(128, kMlpCtasPerSm) mlp_infer_kernel(const flo
     {
         const uint32_t *g = reinterpret_cast<const uint32_t *>(net.w1);
         uint32_t *d = reinterpret_cast<uint32_t *>(sm + MlpSmem::W1);
-        constexpr int n4 = (MlpSmem::A1 - MlpSmem::W1) / 4;  // w1, w2, w3 are contiguous in both
-        static_assert(sizeof(net.w1) + sizeof(net.w2) + sizeof(net.w3) == MlpSmem::A1 - MlpSmem::W1, "weights");
+        constexpr int n4 = (MlpSmem::A1 - MlpSmem::W1) / 4;  // w1 and w2 are contiguous in both
+        static_assert(sizeof(net.w1) + sizeof(net.w2) == MlpSmem::A1 - MlpSmem::W1, "weights");
         for (int i = tid; i < n4; i += 128)
             d[i] = g[i];
     }
-    // the constant columns of this thread's operand rows: 1 after the values, then zeros
-    const uint32_t one_lo = 0x3C00u;  // FP16 1.0 in the low half
-    store_chunk_f16(a1, tid, kMlpIn, 128, one_lo, 0u, 0u, 0u);
-    store_chunk_f16(a1, tid, kMlpIn + 8, 128, 0u, 0u, 0u, 0u);
-    store_chunk_f16(a2, tid, kMlpHidden, 128, one_lo, 0u, 0u, 0u);
-    store_chunk_f16(a2, tid, kMlpHidden + 8, 128, 0u, 0u, 0u, 0u);
     mbar_init_if(leader, bar);
     fence_mbar_init_if(leader);
     __syncwarp();
     if (warp == 0)
-        tmem_alloc_warp(tmem_slot, 32);  // 32 FP32 columns, reused by the three layers
+        tmem_alloc_warp(tmem_slot, 32);  // 32 FP32 columns: layer 1, then layer 2
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     cta_sync();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
     const uint32_t lane_base = uint32_t(warp * 32) << 16;
-    constexpr uint32_t idesc_h = umma_idesc_f16_f32<128, kMlpHidden>();
-    constexpr uint32_t idesc_o = umma_idesc_f16_f32<128, kMlpN3>();
+    constexpr uint32_t idesc = umma_idesc_f16_f32<128, kMlpHidden>();
     unsigned phase = 0;
     bool failed = false;   // warp 0's MMA wait gave up
     bool aborted = false;  // uniform: from the barrier's OR-reduction
     // One layer: a barrier (the operand is written, the previous
     // accumulators are read), the K-steps (16 each) and their commit issued by
-    // one thread, the completion awaited by warp 0 alone (bounded) while the
-    // other warps sleep in the second barrier, whose OR-reduction tells every
-    // thread whether the wait gave up (false: stop).
-    auto layer = [&](const __half *a, const __half *w, uint32_t lbo_w, int ksteps, uint32_t idesc) {
+    // one thread, the completion awaited by warp 0 alone (bounded, sleeping)
+    // while the other warps sleep in the second barrier, whose OR-reduction
+    // tells every thread whether the wait gave up (false: stop).
+    auto layer = [&](const __half *a, const __half *w, int ksteps) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         tc_fence_before();
         cta_sync();
         tc_fence_after();
         for (int s = 0; s < ksteps; s++)
             umma_f16_if(leader, tmem, umma_desc(a + s * MlpSmem::LBO_A, MlpSmem::LBO_A, MlpSmem::SBO),
-                        umma_desc(w + s * lbo_w, lbo_w, MlpSmem::SBO), idesc, s > 0);
+                        umma_desc(w + s * MlpSmem::LBO_W, MlpSmem::LBO_W, MlpSmem::SBO), idesc, s > 0);
         umma_commit_if(leader, bar);
-        if (warp == 0 && !mbar_wait_bounded(bar, phase, timeout_ns)) {
+        if (warp == 0 && !mbar_wait_sleep_bounded(bar, phase, timeout_ns)) {
             if (leader)
                 atomicOr(err, ERR_MMA_TIMEOUT);
             failed = true;
@@ -376,19 +381,6 @@ __global__ void __launch_bounds__(128, kMlpCtasPerSm) mlp_infer_kernel(const flo
         }
         tc_fence_after();
         return true;
-    };
-    // accumulators (bias included) -> GELU in FP16 -> the activation operand
-    auto activate = [&]() {
-        float z[kMlpHidden];
-        tmem_ld_32cols(tmem + lane_base, z);
-#pragma unroll
-        for (int c = 0; c < kMlpHidden / 8; c++) {
-            uint32_t p[4];
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-                p[j] = gelu_f16x2(pack_f16x2_sat(z[8 * c + 2 * j], z[8 * c + 2 * j + 1]));
-            store_chunk_f16(a2, tid, 8 * c, 128, p[0], p[1], p[2], p[3]);
-        }
     };
 
     const size_t tiles = (N + 127) / 128;
@@ -440,15 +432,31 @@ __global__ void __launch_bounds__(128, kMlpCtasPerSm) mlp_infer_kernel(const flo
         }
         // each layer starts at a barrier: the threads have read the previous
         // layer's accumulators (tcgen05.wait::ld) and written its operand
-        if (!layer(a1, w1, MlpSmem::LBO_W, kMlpK1 / 16, idesc_h))  // 16 + 1 -> 32
+        if (!layer(a1, w1, kMlpIn / 16))  // 16 -> 32
             break;
-        activate();
-        if (!layer(a2, w2, MlpSmem::LBO_W, kMlpK2 / 16, idesc_h))  // 32 + 1 -> 32
+        float z[kMlpHidden];
+        tmem_ld_32cols(tmem + lane_base, z);
+#pragma unroll
+        for (int c = 0; c < kMlpHidden / 8; c++) {
+            uint32_t p[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int i = 8 * c + 2 * j;
+                p[j] = gelu_f16x2(pack_f16x2_sat(z[i] + net.b1[i], z[i + 1] + net.b1[i + 1]));
+            }
+            store_chunk_f16(a2, tid, 8 * c, 128, p[0], p[1], p[2], p[3]);
+        }
+        if (!layer(a2, w2, kMlpHidden / 16))  // 32 -> 32
             break;
-        activate();
-        if (!layer(a2, w3, MlpSmem::LBO_W3, kMlpK2 / 16, idesc_o))  // 32 + 1 -> y
-            break;
-        const float y = tmem_ld_1col(tmem + lane_base);
+        tmem_ld_32cols(tmem + lane_base, z);
+        float y = net.b3;
+#pragma unroll
+        for (int i = 0; i < kMlpHidden; i += 2) {
+            const uint32_t g = gelu_f16x2(pack_f16x2_sat(z[i] + net.b2[i], z[i + 1] + net.b2[i + 1]));
+            const float2 h = __half22float2(*reinterpret_cast<const __half2 *>(&g));
+            y = fmaf(net.w3[i], h.x, y);
+            y = fmaf(net.w3[i + 1], h.y, y);
+        }
         if (valid) {
             if constexpr (RAW_Y)
                 out[node] = y;

@@ -58,18 +58,19 @@ def _h(a):
 
 def forward(p, feats, fp16=False):
     """Network output y [n]; fp16=True follows the tensor-core path's
-    roundings (accumulation in FP64): standardised inputs, weights and biases
-    in FP16, each layer's pre-activation rounded to FP16 before the GELU and
-    the activation rounded to FP16 after it.  (The device evaluates the GELU
-    in FP16 arithmetic, which this model rounds only once.)"""
+    roundings (accumulation in FP64): standardised inputs and the weights of
+    the two hidden layers in FP16, biases added in FP32, each hidden layer's
+    pre-activation rounded to FP16 before the GELU and its activation rounded
+    to FP16 after it, the output layer in FP32.  (The device evaluates the
+    GELU in FP16 arithmetic, which this model rounds only once.)"""
     x = (np.asarray(feats, np.float64) - p["in_mean"]) * p["in_scale"]
     w1, w2, w3, b1, b2, b3 = p["w1"], p["w2"], p["w3"], p["b1"], p["b2"], p["b3"]
     if not fp16:
         h1 = gelu(x @ w1.T + b1)
         return gelu(h1 @ w2.T + b2) @ w3 + b3
-    h1 = _h(gelu(_h(_h(x) @ _h(w1).T + _h(b1))))
-    h2 = _h(gelu(_h(h1 @ _h(w2).T + _h(b2))))
-    return h2 @ _h(w3) + _h(b3)
+    h1 = _h(gelu(_h(_h(x) @ _h(w1).T + b1)))
+    h2 = _h(gelu(_h(h1 @ _h(w2).T + b2)))
+    return h2 @ w3 + b3
 
 
 def gradient(p, feats, targets):

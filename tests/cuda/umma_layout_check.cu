@@ -32,27 +32,23 @@ int check_operand(int rows, int K, uint32_t lbo)
 
 }  // namespace
 
-extern "C" int umma_layout_check(uint32_t *idesc_n32, uint32_t *idesc_n16)
+extern "C" int umma_layout_check(uint32_t *idesc_n32)
 {
     using lbm::MlpSmem;
     *idesc_n32 = lbm::umma_idesc_f16_f32<128, lbm::kMlpHidden>();
-    *idesc_n16 = lbm::umma_idesc_f16_f32<128, lbm::kMlpN3>();
-    if (int e = check_operand(128, lbm::kMlpK1, MlpSmem::LBO_A))
-        return 10 + e;  // layer-1 activations
-    if (int e = check_operand(128, lbm::kMlpK2, MlpSmem::LBO_A))
-        return 20 + e;  // hidden activations
-    if (int e = check_operand(lbm::kMlpHidden, lbm::kMlpK1, MlpSmem::LBO_W))
-        return 30 + e;  // w1 | b1
-    if (int e = check_operand(lbm::kMlpHidden, lbm::kMlpK2, MlpSmem::LBO_W))
-        return 40 + e;  // w2 | b2
-    if (int e = check_operand(lbm::kMlpN3, lbm::kMlpK2, MlpSmem::LBO_W3))
-        return 50 + e;  // w3 | b3
+    if (int e = check_operand(128, lbm::kMlpIn, MlpSmem::LBO_A))
+        return 10 + e;  // layer-1 operand: features
+    if (int e = check_operand(128, lbm::kMlpHidden, MlpSmem::LBO_A))
+        return 20 + e;  // layer-2 operand: hidden activations
+    if (int e = check_operand(lbm::kMlpHidden, lbm::kMlpIn, MlpSmem::LBO_W))
+        return 30 + e;  // w1
+    if (int e = check_operand(lbm::kMlpHidden, lbm::kMlpHidden, MlpSmem::LBO_W))
+        return 40 + e;  // w2
     // shared-memory regions: 128-byte aligned, in order, sized as the operands
-    const int regions[][2] = {{MlpSmem::W1, lbm::kMlpHidden * lbm::kMlpK1 * 2},
-                              {MlpSmem::W2, lbm::kMlpHidden * lbm::kMlpK2 * 2},
-                              {MlpSmem::W3, lbm::kMlpN3 * lbm::kMlpK2 * 2},
-                              {MlpSmem::A1, 128 * lbm::kMlpK1 * 2},
-                              {MlpSmem::A2, 128 * lbm::kMlpK2 * 2}};
+    const int regions[][2] = {{MlpSmem::W1, lbm::kMlpHidden * lbm::kMlpIn * 2},
+                              {MlpSmem::W2, lbm::kMlpHidden * lbm::kMlpHidden * 2},
+                              {MlpSmem::A1, 128 * lbm::kMlpIn * 2},
+                              {MlpSmem::A2, 128 * lbm::kMlpHidden * 2}};
     int end = 0;
     for (const auto &g : regions) {
         if (g[0] % 128 || g[0] < end)
@@ -62,8 +58,7 @@ extern "C" int umma_layout_check(uint32_t *idesc_n32, uint32_t *idesc_n16)
     if (MlpSmem::BAR < end || MlpSmem::BAR % 8 || MlpSmem::BYTES > MlpSmem::LAUNCH_BYTES)
         return 61;
     // the weight block copied into shared memory is the struct's leading bytes
-    if (sizeof(lbm::MlpDevice::w1) + sizeof(lbm::MlpDevice::w2) + sizeof(lbm::MlpDevice::w3) !=
-        size_t(MlpSmem::A1 - MlpSmem::W1))
+    if (sizeof(lbm::MlpDevice::w1) + sizeof(lbm::MlpDevice::w2) != size_t(MlpSmem::A1 - MlpSmem::W1))
         return 62;
     return 0;
 }

@@ -2,8 +2,8 @@
 umma_index is the K-major no-swizzle canonical layout with the shared-memory
 descriptors' strides for every operand shape the inference kernel uses, the
 shared-memory regions are aligned and disjoint, and the instruction
-descriptors have the documented values (kind::f16, FP32 accumulator, M = 128,
-N = 32 and 16).  The host code of tests/cuda/umma_layout_check.cu runs
+descriptor has the documented value (kind::f16, FP32 accumulator, M = 128,
+N = 32).  The host code of tests/cuda/umma_layout_check.cu runs
 without a GPU."""
 import ctypes
 import os
@@ -25,12 +25,12 @@ def checker(tmp_path_factory):
                     "-I" + os.path.join(ROOT, "cudalbm_b200", "csrc"), "-I" + os.path.join(ROOT, "include"),
                     os.path.join(ROOT, "tests", "cuda", "umma_layout_check.cu"), "-o", out], check=True)
     L = ctypes.CDLL(out)
-    L.umma_layout_check.argtypes = [ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]
+    L.umma_layout_check.argtypes = [ctypes.POINTER(ctypes.c_uint32)]
     return L
 
 
 def test_operand_layouts_and_descriptors(checker):
-    n32, n16 = ctypes.c_uint32(), ctypes.c_uint32()
-    assert checker.umma_layout_check(ctypes.byref(n32), ctypes.byref(n16)) == 0
+    n32 = ctypes.c_uint32()
+    assert checker.umma_layout_check(ctypes.byref(n32)) == 0
     # D = FP32 (bit 4), N >> 3 at bit 17, M >> 4 at bit 24
-    assert n32.value == 0x08080010 and n16.value == 0x08040010
+    assert n32.value == 0x08080010
