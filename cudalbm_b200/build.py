@@ -114,12 +114,14 @@ def build_executables(force: bool = False) -> list:
     return out
 
 
-def build_oracle() -> None:
-    """CPU oracle (test infrastructure) and, where the reference sources are
-    present, the reference executables used as the parity checker."""
+def build_oracle(reference_dir: str | None = None) -> None:
+    """CPU oracle (test infrastructure) and, when a checkout of the reference
+    is named (argument, else the LBM_REFERENCE_DIR environment variable), the
+    reference executables used as the parity checker.  Without one, the
+    reference binaries are not built and the tests that need them skip."""
     _run(["make", "-s", "-f", os.path.join(ROOT, "oracle", "Makefile")])
-    ref = os.environ.get("LBM_REFERENCE_DIR", "/root/reference")
-    if os.path.isdir(os.path.join(ref, "applications")):
+    ref = reference_dir or os.environ.get("LBM_REFERENCE_DIR")
+    if ref and os.path.isdir(os.path.join(ref, "applications")):
         _run(["make", "-s", "-f", os.path.join(ROOT, "oracle", "Makefile.ref"), f"REF={ref}"])
 
 
