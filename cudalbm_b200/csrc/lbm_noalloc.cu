@@ -17,6 +17,7 @@
 // but all calls share the array: calls that overlap on the GPU (from two
 // streams, or from host threads without ordering between them) race and must
 // be serialised by the caller.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -100,13 +101,49 @@ __global__ void __launch_bounds__(kThreads) final_sum(Partial *scratch, unsigned
         scratch[kMaxPartials] = p;
 }
 
-// Device address of g_partials, looked up once per device with that device
-// current (the name g_partials in host code is only a host-side stand-in).
+// Context identity: cuCtxGetCurrent and cuCtxGetId from the driver (by entry
+// point, so that the library needs no link against libcuda).  A context id is
+// unique for the life of the process, unlike the CUcontext handle value.
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+
+bool current_context_id(unsigned long long *id)
+{
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<CtxGetCurrentFn>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<CtxGetIdFn>(p);
+    });
+    CUcontext ctx = nullptr;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx)
+        return false;
+    return get_id(ctx, id) == CUDA_SUCCESS;
+}
+
+// Device address of g_partials (the name g_partials in host code is only a
+// host-side stand-in).  It is looked up with the device current, once per
+// device and context: the cache entry is keyed on the context's id, so after
+// the device's context is reset (cudaDeviceReset, or a host framework
+// recreating the primary context, which reloads this module) the next call
+// looks the address up again instead of using the old one.
 Partial *scratch_for_current_device(lbm_status *st)
 {
     constexpr int kMaxDevices = 64;
+    struct Entry {
+        unsigned long long ctx;
+        Partial *addr;
+    };
     static std::mutex mu;
-    static Partial *addr[kMaxDevices] = {};
+    static Entry cache[kMaxDevices] = {};
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
@@ -114,17 +151,26 @@ Partial *scratch_for_current_device(lbm_status *st)
         return nullptr;
     }
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_partials);
-        if (e != cudaSuccess || !p) {
-            *st = fail(LBM_ERR_CUDA, std::string("cudaGetSymbolAddress(g_partials): ") + cudaGetErrorString(e));
-            return nullptr;
-        }
-        addr[dev] = static_cast<Partial *>(p);
+    unsigned long long ctx = 0;
+    const bool known = current_context_id(&ctx);
+    if (known && cache[dev].addr && cache[dev].ctx == ctx) {
+        *st = LBM_OK;
+        return cache[dev].addr;
     }
+    // set-up: look the address up in the current context (this also makes the
+    // device's primary context current if the thread had none yet)
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_partials);
+    if (e != cudaSuccess || !p) {
+        *st = fail(LBM_ERR_CUDA, std::string("cudaGetSymbolAddress(g_partials): ") + cudaGetErrorString(e));
+        return nullptr;
+    }
+    if (current_context_id(&ctx))
+        cache[dev] = {ctx, static_cast<Partial *>(p)};
+    else
+        cache[dev] = {0, nullptr};  // context not identifiable: look up again on every call
     *st = LBM_OK;
-    return addr[dev];
+    return static_cast<Partial *>(p);
 }
 
 }  // namespace

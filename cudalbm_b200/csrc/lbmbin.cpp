@@ -130,29 +130,54 @@ FieldFileHeader read_field_header(const std::string &path)
     return h;
 }
 
-std::vector<float> read_field_by_name(const std::string &path, const std::string &name)
+namespace {
+// Position of field `name` among the file's fields.
+size_t field_index(const FieldFileHeader &h, const std::string &path, const std::string &name)
 {
-    const FieldFileHeader h = read_field_header(path);
     size_t k = 0;
     while (k < h.names.size() && h.names[k] != name)
         k++;
     if (k == h.names.size())
         throw CaseError("Field " + name + " not found in " + path);
+    return k;
+}
+
+template <typename T>
+std::vector<T> read_field_as(const std::string &path, const std::string &name)
+{
+    const FieldFileHeader h = read_field_header(path);
+    const size_t k = field_index(h, path, name);
     const uint64_t n = h.nx * h.ny * h.nz;
     std::ifstream in(path, std::ios::binary);
     in.seekg(std::streamoff(h.data_offset + k * n * uint64_t(h.scalar_bytes)));
-    std::vector<float> out(n);
-    if (h.scalar_bytes == 4) {
-        in.read(reinterpret_cast<char *>(out.data()), std::streamsize(n * 4));
+    std::vector<T> out(n);
+    if (h.scalar_bytes == int(sizeof(T))) {
+        in.read(reinterpret_cast<char *>(out.data()), std::streamsize(n * sizeof(T)));
+    } else if (h.scalar_bytes == 4) {
+        std::vector<float> tmp(n);
+        in.read(reinterpret_cast<char *>(tmp.data()), std::streamsize(n * 4));
+        for (uint64_t i = 0; i < n; i++)
+            out[i] = T(tmp[i]);
     } else {
         std::vector<double> tmp(n);
         in.read(reinterpret_cast<char *>(tmp.data()), std::streamsize(n * 8));
         for (uint64_t i = 0; i < n; i++)
-            out[i] = float(tmp[i]);
+            out[i] = T(tmp[i]);
     }
     if (!in)
         throw CaseError("Truncated field file: " + path);
     return out;
+}
+}  // namespace
+
+std::vector<float> read_field_by_name(const std::string &path, const std::string &name)
+{
+    return read_field_as<float>(path, name);
+}
+
+std::vector<double> read_field_by_name_f64(const std::string &path, const std::string &name)
+{
+    return read_field_as<double>(path, name);
 }
 
 }  // namespace lbm

@@ -36,5 +36,7 @@ FieldFileHeader read_field_header(const std::string &path);
 
 // One field (tiled order) converted to float.
 std::vector<float> read_field_by_name(const std::string &path, const std::string &name);
+// One field (tiled order) as double: exact for 32- and 64-bit files alike.
+std::vector<double> read_field_by_name_f64(const std::string &path, const std::string &name);
 
 }  // namespace lbm

@@ -12,7 +12,16 @@
 // queues the steps between two such events without synchronising the device.
 //
 // Optional file b200Options (ignored by the reference) may set
-// `meanPrecision 64;` for double-precision running means.
+//   meanPrecision 64;   double-precision running means;
+//   restoreMeans 1;     on restart, read the function-object fields saved at
+//                       the restart time (momentsMean, S, SMean, k, kMean --
+//                       those the functionObjects list enables) back into the
+//                       device accumulators, so that a restarted run continues
+//                       its running means exactly as an uninterrupted run.
+// Without restoreMeans the running means restart from zero while their count
+// 1/(t+1) keeps the absolute step, as in the reference
+// (src/functionObjects/strainRateTensor.cuh:331; src/array/hostArray.cuh:264-276
+// restores the moments only).
 #include <algorithm>
 #include <array>
 #include <chrono>
@@ -114,6 +123,40 @@ struct Saver {
     }
 };
 
+// The function-object fields saved at step t, read back into the handle's
+// accumulators (the files' names and field names as Saver::all writes them;
+// 32- or 64-bit files, any mean precision of the handle).
+void restore_function_objects(lbm_handle *h, uint32_t fo, uint64_t t, uint64_t N)
+{
+    const std::vector<std::string> S = {"S_xx", "S_xy", "S_xz", "S_yy", "S_yz", "S_zz"};
+    struct Item {
+        uint32_t bit;
+        lbm_field_set set;
+        std::string prefix;
+        std::vector<std::string> names;
+    };
+    const Item items[] = {{LBM_FO_MOMENTSMEAN, LBM_FIELDS_MOMENTSMEAN, "momentsMean", with_suffix(kMoments, "Mean")},
+                          {LBM_FO_S, LBM_FIELDS_S, "S", S},
+                          {LBM_FO_SMEAN, LBM_FIELDS_SMEAN, "SMean", with_suffix(S, "Mean")},
+                          {LBM_FO_K, LBM_FIELDS_K, "k", {"k"}},
+                          {LBM_FO_KMEAN, LBM_FIELDS_KMEAN, "kMean", {"kMean"}}};
+    for (const Item &it : items) {
+        if (!(fo & it.bit))
+            continue;
+        const std::string file = it.prefix + "_" + std::to_string(t) + ".LBMBin";
+        if (!std::filesystem::exists(file))
+            throw lbm::CaseError("restoreMeans: " + file + " not found (saved function objects are needed at the restart time)");
+        std::vector<double> all(it.names.size() * N);
+        for (size_t f = 0; f < it.names.size(); f++) {
+            const std::vector<double> v = lbm::read_field_by_name_f64(file, it.names[f]);
+            if (v.size() != N)
+                throw lbm::CaseError("Field size mismatch in " + file);
+            std::copy(v.begin(), v.end(), all.begin() + f * N);
+        }
+        check(lbm_write_fields(h, it.set, all.data(), all.size(), LBM_F64, LBM_ORDER_TILED));
+    }
+}
+
 std::string hms(long long s)
 {
     std::ostringstream o;
@@ -147,10 +190,15 @@ int run(int argc, char **argv)
     cfg.u_inf = pc.u_inf;
     cfg.function_objects = lbm::read_function_objects(".");
     cfg.start_step = int64_t(latest);
+    bool restore_means = false;
     if (std::filesystem::exists("b200Options")) {
         const lbm::Lines L = lbm::read_lines("b200Options");
         try {
             cfg.mean_bits = std::stoi(lbm::parameter_string(L, "meanPrecision"));
+        } catch (const lbm::CaseError &) {
+        }
+        try {
+            restore_means = std::stoi(lbm::parameter_string(L, "restoreMeans")) != 0;
         } catch (const lbm::CaseError &) {
         }
     }
@@ -168,8 +216,11 @@ int run(int argc, char **argv)
                 throw lbm::CaseError("Field size mismatch in " + file);
             std::copy(v.begin(), v.end(), all.begin() + f * N);
         }
-        // running means restart from zero, as in the reference (their count keeps the absolute step)
         check(lbm_write_fields(h, LBM_FIELDS_MOMENTS, all.data(), all.size(), LBM_F32, LBM_ORDER_TILED));
+        // running means: from the saved files with restoreMeans, else from
+        // zero as in the reference (their count keeps the absolute step)
+        if (restore_means)
+            restore_function_objects(h, cfg.function_objects, latest, N);
     } else {
         const std::array<float, 70> region = lbm::read_initial_conditions(".");
         check(lbm_init_regions(h, region.data()));

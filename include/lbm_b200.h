@@ -193,10 +193,12 @@ lbm_status lbm_autotune(lbm_handle *h, int32_t trial_steps, lbm_tuning *out);
  * partial sum per 16384 nodes) is a fixed 1.5 MiB device array of the library,
  * present on every GPU that loads it, so at most 2^30 nodes are accepted
  * (LBM_ERR_ARG beyond).  Sums use a fixed order, so repeated calls agree bit
- * for bit.  The first call on a device looks up the array's address; make it
- * before any stream capture.  Calls share the array: calls that overlap on the
- * GPU race and must be serialised.  `stream` is a cudaStream_t (NULL: default
- * stream); the call returns after the result is on the host.
+ * for bit.  The first call on a device (and the first after that device's
+ * context has been reset) looks up the array's address; make that first call
+ * before any stream capture begins.  Each call copies the three sums to host
+ * memory and waits for `stream` to finish (cudaStreamSynchronize) before it
+ * returns.  Calls share the array: calls that overlap on the GPU race and must
+ * be serialised.  `stream` is a cudaStream_t (NULL: default stream).
  * No counterpart in the reference, which has no allocation-free entry point. */
 lbm_status lbm_reduce_moments_noalloc(const float *moments, uint64_t nodes, double out[3], void *stream);
 

@@ -75,3 +75,55 @@ def test_command_line_and_case_errors():
     os.remove(os.path.join(d, "latticeMesh"))
     r = run(exe, d, check=False)
     assert r.returncode != 0 and "latticeMesh file not opened" in r.stderr
+
+
+FO_ALL = ("S", "SMean", "k", "kMean", "momentsMean")
+FO_PREFIXES = ("lidDrivenCavity", "S", "SMean", "k", "kMean", "momentsMean")
+
+
+def restart_pair(q, opts):
+    """Run 0..40 in one go, and 0..20 then a restart to 40, with the same
+    b200Options; returns the two case directories."""
+    spec = casefiles.CaseSpec(nx=16, ny=16, nz=24, Re=200.0, u_inf=0.05, n_steps=41, save_interval=20,
+                              info_interval=20, function_objects=FO_ALL, extra_files=opts)
+    one, two = tempfile.mkdtemp(), tempfile.mkdtemp()
+    casefiles.write_case(one, spec)
+    casefiles.write_case(two, casefiles.CaseSpec(**{**spec.__dict__, "n_steps": 21}))
+    exe = os.path.join(BIN, f"momentBasedD3Q{q}")
+    run(exe, one)
+    run(exe, two)
+    casefiles.write_case(two, spec)  # extend nTimeSteps, keep the files of t = 20
+    out = run(exe, two)
+    assert "latestTime = 20" in out.stdout
+    return one, two
+
+
+@pytest.mark.parametrize("q", [19, 27])
+@pytest.mark.parametrize("precision", [32, 64])
+def test_restart_with_restored_means_continues_like_one_run(q, precision):
+    """b200Options `restoreMeans 1;`: the running means (FP32 or FP64
+    accumulators) and S/k saved at the restart time are read back, so every
+    file of the restarted run -- moments and all five function objects, at the
+    restart step and at the end -- is byte-identical to the uninterrupted run's."""
+    one, two = restart_pair(q, {"b200Options": f"meanPrecision {precision};\nrestoreMeans 1;\n"})
+    for t in (20, 40):
+        for p in FO_PREFIXES:
+            f = f"{p}_{t}.LBMBin"
+            assert open(os.path.join(one, f), "rb").read() == open(os.path.join(two, f), "rb").read(), f
+    if precision == 64:
+        h = lbmbin.read(os.path.join(two, "SMean_40.LBMBin"))
+        assert h.data.dtype == np.float64
+
+
+def test_restart_without_restored_means_keeps_the_reference_behaviour():
+    """Default (the reference's rule): the moments continue exactly, the
+    running means restart from zero with 1/(t+1) at the absolute step."""
+    one, two = restart_pair(19, {})
+    a = lbmbin.read(os.path.join(one, "lidDrivenCavity_40.LBMBin")).data
+    b = lbmbin.read(os.path.join(two, "lidDrivenCavity_40.LBMBin")).data
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    ma = lbmbin.read(os.path.join(one, "kMean_40.LBMBin")).data
+    mb = lbmbin.read(os.path.join(two, "kMean_40.LBMBin")).data
+    assert not np.array_equal(ma, mb)
+    # after the restart the means hold only steps 20..39, weighted by 1/(t+1)
+    assert np.abs(mb).max() < np.abs(ma).max()
