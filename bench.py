@@ -197,6 +197,39 @@ def cpu_baseline(w, budget_s: float = 12.0):
             "sample": f"FP64 OpenMP oracle, {w['desc']}, {steps} steps after 1 untimed"}
 
 
+def link_ceiling(device: int):
+    """Pinned host<->device copy rate of this box (GB/s): the best of three
+    plain 1 GiB cudaMemcpyAsync each way, timed with CUDA events (torch is the
+    plumbing here; the library is not involved)."""
+    try:
+        import torch
+
+        n = 1 << 30
+        dev = torch.device("cuda", device)
+        torch.cuda.set_device(dev)
+        h = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+        d = torch.empty(n, dtype=torch.uint8, device=dev)
+        out = {}
+        for key, fn in (("h2d", lambda: d.copy_(h, non_blocking=True)), ("d2h", lambda: h.copy_(d, non_blocking=True))):
+            best = None
+            for _ in range(3):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize(dev)
+                e0.record()
+                fn()
+                e1.record()
+                torch.cuda.synchronize(dev)
+                ms = e0.elapsed_time(e1)
+                best = ms if best is None else min(best, ms)
+            out[key] = round(n / (best / 1e3) / 1e9, 2)
+        del h, d
+        torch.cuda.empty_cache()
+        return out
+    except Exception as exc:  # reported, never silent
+        log(f"link ceiling not measured: {exc!r}")
+        return None
+
+
 L2_BYTES = 126e6
 
 
@@ -254,20 +287,25 @@ def run_ours(args, w):
     outs = {fs: _lib.PinnedArray((NVARS[fs], nz, ny, nx), np.float64 if (w["mean_bits"] == 64 and "Mean" in fs)
                                  else np.float32) for fs in ("moments",) + tuple(w["fo"])}
     mon = _lib.PinnedArray((args.steps,), np.dtype(_lib.MONITOR_DTYPE))
+    link = link_ceiling(local)
     barrier()
     cav.synchronize()
     t0 = time.perf_counter()
     cav.write(state.array)
+    t1 = time.perf_counter()
     for s in range(args.steps):
         cav.step_monitored(1, out=mon.array[s:s + 1])
+    cav.synchronize()
+    t2 = time.perf_counter()
     for fs, buf in outs.items():
         cav.read(fs, out=buf.array)
-    t1 = time.perf_counter()
+    t3 = time.perf_counter()
     barrier()
-    e2e_s = max_over_ranks(t1 - t0)
+    e2e_s = max_over_ranks(t3 - t0)
     e2e = world * nodes * args.steps / e2e_s / 1e6
     h2d = 10 * nodes * 4
     d2h = sum(b.array.nbytes for b in outs.values())
+    copy_gbs = {"h2d": round(h2d / (t1 - t0) / 1e9, 2), "d2h": round(d2h / (t3 - t2) / 1e9, 2)}
     red = {"mass": float(mon.array[-1]["mass"]), "nonfinite": int(mon.array["nonfinite"].max())}
     cav.close()
     group.close()
@@ -303,7 +341,11 @@ def run_ours(args, w):
                 "d2h_bytes_per_step": round(24 + d2h / args.steps),
                 "what": "lbm_write_fields (pinned h2d of the state) + K x lbm_step_monitored (each step's 24 B "
                         "FP64 mass/energy/non-finite sums copied back) + lbm_read_fields of moments and "
-                        "function objects"},
+                        "function objects",
+                "seconds": {"h2d": round(t1 - t0, 5), "steps": round(t2 - t1, 5), "d2h": round(t3 - t2, 5)},
+                "copy_gbs": copy_gbs, "link_gbs": link,
+                "copy_frac_of_link": ({k: round(copy_gbs[k] / link[k], 3) for k in ("h2d", "d2h")}
+                                      if link else None)},
         "gpu_launches": int(launches),
         "clocks": clocks,
         "check": {"mass_last_step": red["mass"], "nonfinite_max": red["nonfinite"]},

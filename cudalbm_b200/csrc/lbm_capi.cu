@@ -346,6 +346,124 @@ lbm_status ensure_scratch(lbm_handle *h, size_t bytes)
     return LBM_OK;
 }
 
+// How one field set moves between host values and the device buffer.
+struct Xfer {
+    size_t hsz;   // bytes per host value
+    bool direct;  // one plain copy: same order, type and values on both sides
+};
+Xfer xfer_of(const lbm_handle *h, lbm_field_set set, lbm_dtype dtype, int is_double, lbm_order order)
+{
+    const size_t hsz = dtype == LBM_F64 ? 8 : 4;
+    const bool moments = set == LBM_FIELDS_MOMENTS;
+    const size_t dsz = moments ? h->esz : (is_double ? 8 : 4);
+    return {hsz, order == LBM_ORDER_GLOBAL && hsz == dsz && (!moments || h->storage == 0)};
+}
+
+// The copy stream, its events and two scratch halves of `half` bytes.
+lbm_status ensure_xfer(lbm_handle *h, size_t half)
+{
+    if (!h->xstream)
+        LBM_CUDA(cudaStreamCreateWithFlags(&h->xstream, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; b++) {
+        if (!h->xe_copied[b])
+            LBM_CUDA(cudaEventCreateWithFlags(&h->xe_copied[b], cudaEventDisableTiming));
+        if (!h->xe_converted[b])
+            LBM_CUDA(cudaEventCreateWithFlags(&h->xe_converted[b], cudaEventDisableTiming));
+    }
+    return ensure_scratch(h, 2 * half);
+}
+
+dim3 grid_1d(size_t N);
+
+// Field v of a set: host values in `src` (order and type of the call) ->
+// device field, on the handle stream.
+lbm_status convert_in(lbm_handle *h, lbm_field_set set, lbm_dtype dtype, int is_double, void *dptr, int v,
+                      const void *src, int tiled)
+{
+    const int nx = int(h->cfg.nx), ny = int(h->cfg.ny), nz = int(h->cfg.nz);
+    const dim3 g = grid_1d(h->N);
+    cudaStream_t st = h->stream;
+    const bool f64 = dtype == LBM_F64;
+    if (set == LBM_FIELDS_MOMENTS) {
+        // moments go through the storage format (FP32 / FP16 / BF16)
+        char *dst = static_cast<char *>(dptr) + size_t(v) * h->N * h->esz;
+        if (h->storage == 1) {
+            if (f64)
+                moment_in_kernel<<<g, 256, 0, st>>>(reinterpret_cast<__half *>(dst), static_cast<const double *>(src), v, nx, ny, nz, tiled);
+            else
+                moment_in_kernel<<<g, 256, 0, st>>>(reinterpret_cast<__half *>(dst), static_cast<const float *>(src), v, nx, ny, nz, tiled);
+        } else if (h->storage == 2) {
+            if (f64)
+                moment_in_kernel<<<g, 256, 0, st>>>(reinterpret_cast<__nv_bfloat16 *>(dst), static_cast<const double *>(src), v, nx, ny, nz, tiled);
+            else
+                moment_in_kernel<<<g, 256, 0, st>>>(reinterpret_cast<__nv_bfloat16 *>(dst), static_cast<const float *>(src), v, nx, ny, nz, tiled);
+        } else {
+            if (f64)
+                moment_in_kernel<<<g, 256, 0, st>>>(reinterpret_cast<float *>(dst), static_cast<const double *>(src), v, nx, ny, nz, tiled);
+            else
+                moment_in_kernel<<<g, 256, 0, st>>>(reinterpret_cast<float *>(dst), static_cast<const float *>(src), v, nx, ny, nz, tiled);
+        }
+    } else if (f64) {
+        if (is_double)
+            gather_in_kernel<double, double><<<g, 256, 0, st>>>(static_cast<double *>(dptr) + v * h->N, static_cast<const double *>(src), nx, ny, nz, tiled);
+        else
+            gather_in_kernel<double, float><<<g, 256, 0, st>>>(static_cast<float *>(dptr) + v * h->N, static_cast<const double *>(src), nx, ny, nz, tiled);
+    } else {
+        if (is_double)
+            gather_in_kernel<float, double><<<g, 256, 0, st>>>(static_cast<double *>(dptr) + v * h->N, static_cast<const float *>(src), nx, ny, nz, tiled);
+        else
+            gather_in_kernel<float, float><<<g, 256, 0, st>>>(static_cast<float *>(dptr) + v * h->N, static_cast<const float *>(src), nx, ny, nz, tiled);
+    }
+    LBM_CUDA(cudaGetLastError());
+    h->launches += 1;
+    return LBM_OK;
+}
+
+// Field v of a set: device field -> host values in `dst` (order and type of
+// the call), on the handle stream.
+lbm_status convert_out(lbm_handle *h, lbm_field_set set, lbm_dtype dtype, int is_double, const void *dptr, int v,
+                       void *dst, int tiled)
+{
+    const int nx = int(h->cfg.nx), ny = int(h->cfg.ny), nz = int(h->cfg.nz);
+    const dim3 g = grid_1d(h->N);
+    cudaStream_t st = h->stream;
+    const bool f64 = dtype == LBM_F64;
+    const bool moments = set == LBM_FIELDS_MOMENTS;
+    const size_t dsz = moments ? h->esz : (is_double ? 8 : 4);
+    const char *src = static_cast<const char *>(dptr) + size_t(v) * h->N * dsz;
+    if (moments) {
+        if (h->storage == 1) {
+            if (f64)
+                moment_out_kernel<<<g, 256, 0, st>>>(static_cast<double *>(dst), reinterpret_cast<const __half *>(src), v, nx, ny, nz, tiled);
+            else
+                moment_out_kernel<<<g, 256, 0, st>>>(static_cast<float *>(dst), reinterpret_cast<const __half *>(src), v, nx, ny, nz, tiled);
+        } else if (h->storage == 2) {
+            if (f64)
+                moment_out_kernel<<<g, 256, 0, st>>>(static_cast<double *>(dst), reinterpret_cast<const __nv_bfloat16 *>(src), v, nx, ny, nz, tiled);
+            else
+                moment_out_kernel<<<g, 256, 0, st>>>(static_cast<float *>(dst), reinterpret_cast<const __nv_bfloat16 *>(src), v, nx, ny, nz, tiled);
+        } else {
+            if (f64)
+                moment_out_kernel<<<g, 256, 0, st>>>(static_cast<double *>(dst), reinterpret_cast<const float *>(src), v, nx, ny, nz, tiled);
+            else
+                moment_out_kernel<<<g, 256, 0, st>>>(static_cast<float *>(dst), reinterpret_cast<const float *>(src), v, nx, ny, nz, tiled);
+        }
+    } else if (f64) {
+        if (is_double)
+            scatter_out_kernel<double, double><<<g, 256, 0, st>>>(static_cast<double *>(dst), reinterpret_cast<const double *>(src), nx, ny, nz, tiled);
+        else
+            scatter_out_kernel<float, double><<<g, 256, 0, st>>>(static_cast<double *>(dst), reinterpret_cast<const float *>(src), nx, ny, nz, tiled);
+    } else {
+        if (is_double)
+            scatter_out_kernel<double, float><<<g, 256, 0, st>>>(static_cast<float *>(dst), reinterpret_cast<const double *>(src), nx, ny, nz, tiled);
+        else
+            scatter_out_kernel<float, float><<<g, 256, 0, st>>>(static_cast<float *>(dst), reinterpret_cast<const float *>(src), nx, ny, nz, tiled);
+    }
+    LBM_CUDA(cudaGetLastError());
+    h->launches += 1;
+    return LBM_OK;
+}
+
 dim3 grid_1d(size_t N)
 {
     return dim3(unsigned(std::min<size_t>((N + 255) / 256, size_t(148) * 16)));
@@ -454,6 +572,14 @@ void destroy_handle(lbm_handle *h)
         cudaGraphExecDestroy(h->steps_graph);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->xstream) {
+        cudaStreamSynchronize(h->xstream);
+        cudaStreamDestroy(h->xstream);
+    }
+    for (int b = 0; b < 2; b++) {
+        if (h->xe_copied[b]) cudaEventDestroy(h->xe_copied[b]);
+        if (h->xe_converted[b]) cudaEventDestroy(h->xe_converted[b]);
+    }
     if (h->stream && h->own_stream)
         cudaStreamDestroy(h->stream);
     delete h;
@@ -659,48 +785,31 @@ lbm_status lbm_write_fields(lbm_handle *h, lbm_field_set set, const void *host, 
     lbm_status s = field_ptr(h, set, &dptr, &is_double);
     if (s != LBM_OK)
         return s;
-    const size_t hsz = dtype == LBM_F64 ? 8 : 4;
-    if ((s = ensure_scratch(h, h->N * hsz)) != LBM_OK)
+    const Xfer x = xfer_of(h, set, dtype, is_double, order);
+    if (x.direct) {
+        // same values, order and type on both sides: one copy
+        LBM_CUDA(cudaMemcpyAsync(dptr, host, size_t(nv) * h->N * x.hsz, cudaMemcpyHostToDevice, h->stream));
+        LBM_CUDA(cudaStreamSynchronize(h->stream));
+        return LBM_OK;
+    }
+    if ((s = ensure_xfer(h, h->N * x.hsz)) != LBM_OK)
         return s;
-    const int tiled = order == LBM_ORDER_TILED;
+    // field v: host -> scratch half (v & 1) on the copy stream, then the
+    // conversion kernel on the handle stream; the copy of v + 1 overlaps the
+    // conversion of v, and a half is refilled only after its kernel has run
+    LBM_CUDA(cudaEventRecord(h->xe_converted[0], h->stream));
+    LBM_CUDA(cudaEventRecord(h->xe_converted[1], h->stream));
     for (int v = 0; v < nv; v++) {
-        const char *src = static_cast<const char *>(host) + size_t(v) * h->N * hsz;
-        LBM_CUDA(cudaMemcpyAsync(h->scratch, src, h->N * hsz, cudaMemcpyHostToDevice, h->stream));
-        const int nx = int(h->cfg.nx), ny = int(h->cfg.ny), nz = int(h->cfg.nz);
-        const dim3 g = grid_1d(h->N);
-        if (set == LBM_FIELDS_MOMENTS) {
-            // moments go through the storage format (FP32 / FP16 / BF16)
-            char *dst = static_cast<char *>(dptr) + size_t(v) * h->N * h->esz;
-            const void *sc = h->scratch;
-            if (h->storage == 1) {
-                if (dtype == LBM_F64)
-                    moment_in_kernel<<<g, 256, 0, h->stream>>>(reinterpret_cast<__half *>(dst), static_cast<const double *>(sc), v, nx, ny, nz, tiled);
-                else
-                    moment_in_kernel<<<g, 256, 0, h->stream>>>(reinterpret_cast<__half *>(dst), static_cast<const float *>(sc), v, nx, ny, nz, tiled);
-            } else if (h->storage == 2) {
-                if (dtype == LBM_F64)
-                    moment_in_kernel<<<g, 256, 0, h->stream>>>(reinterpret_cast<__nv_bfloat16 *>(dst), static_cast<const double *>(sc), v, nx, ny, nz, tiled);
-                else
-                    moment_in_kernel<<<g, 256, 0, h->stream>>>(reinterpret_cast<__nv_bfloat16 *>(dst), static_cast<const float *>(sc), v, nx, ny, nz, tiled);
-            } else {
-                if (dtype == LBM_F64)
-                    moment_in_kernel<<<g, 256, 0, h->stream>>>(reinterpret_cast<float *>(dst), static_cast<const double *>(sc), v, nx, ny, nz, tiled);
-                else
-                    moment_in_kernel<<<g, 256, 0, h->stream>>>(reinterpret_cast<float *>(dst), static_cast<const float *>(sc), v, nx, ny, nz, tiled);
-            }
-        } else if (dtype == LBM_F64) {
-            if (is_double)
-                gather_in_kernel<double, double><<<g, 256, 0, h->stream>>>(static_cast<double *>(dptr) + v * h->N, static_cast<const double *>(h->scratch), nx, ny, nz, tiled);
-            else
-                gather_in_kernel<double, float><<<g, 256, 0, h->stream>>>(static_cast<float *>(dptr) + v * h->N, static_cast<const double *>(h->scratch), nx, ny, nz, tiled);
-        } else {
-            if (is_double)
-                gather_in_kernel<float, double><<<g, 256, 0, h->stream>>>(static_cast<double *>(dptr) + v * h->N, static_cast<const float *>(h->scratch), nx, ny, nz, tiled);
-            else
-                gather_in_kernel<float, float><<<g, 256, 0, h->stream>>>(static_cast<float *>(dptr) + v * h->N, static_cast<const float *>(h->scratch), nx, ny, nz, tiled);
-        }
-        LBM_CUDA(cudaGetLastError());
-        h->launches += 1;
+        const int b = v & 1;
+        char *half = static_cast<char *>(h->scratch) + size_t(b) * h->N * x.hsz;
+        const char *src = static_cast<const char *>(host) + size_t(v) * h->N * x.hsz;
+        LBM_CUDA(cudaStreamWaitEvent(h->xstream, h->xe_converted[b], 0));
+        LBM_CUDA(cudaMemcpyAsync(half, src, h->N * x.hsz, cudaMemcpyHostToDevice, h->xstream));
+        LBM_CUDA(cudaEventRecord(h->xe_copied[b], h->xstream));
+        LBM_CUDA(cudaStreamWaitEvent(h->stream, h->xe_copied[b], 0));
+        if ((s = convert_in(h, set, dtype, is_double, dptr, v, half, order == LBM_ORDER_TILED)) != LBM_OK)
+            return s;
+        LBM_CUDA(cudaEventRecord(h->xe_converted[b], h->stream));
     }
     LBM_CUDA(cudaStreamSynchronize(h->stream));
     return LBM_OK;
@@ -715,61 +824,40 @@ lbm_status lbm_read_fields(lbm_handle *h, lbm_field_set set, void *host, size_t 
         return fail(LBM_ERR_ARG, "unknown field set");
     if (count != size_t(nv) * h->N)
         return fail(LBM_ERR_ARG, "count must equal nvars * nx * ny * nz");
+    if (order == LBM_ORDER_TILED && (h->cfg.nx % 8 || h->cfg.ny % 8 || h->cfg.nz % 8))
+        return fail(LBM_ERR_ARG, "tiled order needs multiples of 8");
     LBM_CUDA(cudaSetDevice(h->cfg.device));
     void *dptr;
     int is_double;
     lbm_status s = field_ptr(h, set, &dptr, &is_double);
     if (s != LBM_OK)
         return s;
-    const size_t hsz = dtype == LBM_F64 ? 8 : 4;
-    const bool moments = set == LBM_FIELDS_MOMENTS;
-    const size_t dsz = moments ? h->esz : (is_double ? 8 : 4);
-    const int tiled = order == LBM_ORDER_TILED;
-    const bool direct = !tiled && hsz == dsz && (!moments || h->storage == 0);
-    if (!direct && (s = ensure_scratch(h, h->N * hsz)) != LBM_OK)
-        return s;
-    const int nx = int(h->cfg.nx), ny = int(h->cfg.ny), nz = int(h->cfg.nz);
-    const dim3 g = grid_1d(h->N);
-    for (int v = 0; v < nv; v++) {
-        char *dst = static_cast<char *>(host) + size_t(v) * h->N * hsz;
-        const char *src = static_cast<const char *>(dptr) + size_t(v) * h->N * dsz;
-        if (direct) {
-            LBM_CUDA(cudaMemcpyAsync(dst, src, h->N * hsz, cudaMemcpyDeviceToHost, h->stream));
-            continue;
-        }
-        void *sc = h->scratch;
-        if (moments) {
-            if (h->storage == 1) {
-                if (dtype == LBM_F64)
-                    moment_out_kernel<<<g, 256, 0, h->stream>>>(static_cast<double *>(sc), reinterpret_cast<const __half *>(src), v, nx, ny, nz, tiled);
-                else
-                    moment_out_kernel<<<g, 256, 0, h->stream>>>(static_cast<float *>(sc), reinterpret_cast<const __half *>(src), v, nx, ny, nz, tiled);
-            } else if (h->storage == 2) {
-                if (dtype == LBM_F64)
-                    moment_out_kernel<<<g, 256, 0, h->stream>>>(static_cast<double *>(sc), reinterpret_cast<const __nv_bfloat16 *>(src), v, nx, ny, nz, tiled);
-                else
-                    moment_out_kernel<<<g, 256, 0, h->stream>>>(static_cast<float *>(sc), reinterpret_cast<const __nv_bfloat16 *>(src), v, nx, ny, nz, tiled);
-            } else {
-                if (dtype == LBM_F64)
-                    moment_out_kernel<<<g, 256, 0, h->stream>>>(static_cast<double *>(sc), reinterpret_cast<const float *>(src), v, nx, ny, nz, tiled);
-                else
-                    moment_out_kernel<<<g, 256, 0, h->stream>>>(static_cast<float *>(sc), reinterpret_cast<const float *>(src), v, nx, ny, nz, tiled);
-            }
-        } else if (dtype == LBM_F64) {
-            if (is_double)
-                scatter_out_kernel<double, double><<<g, 256, 0, h->stream>>>(static_cast<double *>(sc), reinterpret_cast<const double *>(src), nx, ny, nz, tiled);
-            else
-                scatter_out_kernel<float, double><<<g, 256, 0, h->stream>>>(static_cast<double *>(sc), reinterpret_cast<const float *>(src), nx, ny, nz, tiled);
-        } else {
-            if (is_double)
-                scatter_out_kernel<double, float><<<g, 256, 0, h->stream>>>(static_cast<float *>(sc), reinterpret_cast<const double *>(src), nx, ny, nz, tiled);
-            else
-                scatter_out_kernel<float, float><<<g, 256, 0, h->stream>>>(static_cast<float *>(sc), reinterpret_cast<const float *>(src), nx, ny, nz, tiled);
-        }
-        LBM_CUDA(cudaGetLastError());
-        h->launches += 1;
-        LBM_CUDA(cudaMemcpyAsync(dst, h->scratch, h->N * hsz, cudaMemcpyDeviceToHost, h->stream));
+    const Xfer x = xfer_of(h, set, dtype, is_double, order);
+    if (x.direct) {
+        LBM_CUDA(cudaMemcpyAsync(host, dptr, size_t(nv) * h->N * x.hsz, cudaMemcpyDeviceToHost, h->stream));
+        LBM_CUDA(cudaStreamSynchronize(h->stream));
+        return LBM_OK;
     }
+    if ((s = ensure_xfer(h, h->N * x.hsz)) != LBM_OK)
+        return s;
+    // field v: conversion kernel into scratch half (v & 1) on the handle
+    // stream, then scratch -> host on the copy stream; the conversion of v + 1
+    // overlaps the copy of v, and a half is rewritten only after its copy
+    LBM_CUDA(cudaEventRecord(h->xe_copied[0], h->stream));
+    LBM_CUDA(cudaEventRecord(h->xe_copied[1], h->stream));
+    for (int v = 0; v < nv; v++) {
+        const int b = v & 1;
+        char *half = static_cast<char *>(h->scratch) + size_t(b) * h->N * x.hsz;
+        char *dst = static_cast<char *>(host) + size_t(v) * h->N * x.hsz;
+        LBM_CUDA(cudaStreamWaitEvent(h->stream, h->xe_copied[b], 0));
+        if ((s = convert_out(h, set, dtype, is_double, dptr, v, half, order == LBM_ORDER_TILED)) != LBM_OK)
+            return s;
+        LBM_CUDA(cudaEventRecord(h->xe_converted[b], h->stream));
+        LBM_CUDA(cudaStreamWaitEvent(h->xstream, h->xe_converted[b], 0));
+        LBM_CUDA(cudaMemcpyAsync(dst, half, h->N * x.hsz, cudaMemcpyDeviceToHost, h->xstream));
+        LBM_CUDA(cudaEventRecord(h->xe_copied[b], h->xstream));
+    }
+    LBM_CUDA(cudaStreamSynchronize(h->xstream));
     LBM_CUDA(cudaStreamSynchronize(h->stream));
     return LBM_OK;
 }

@@ -34,6 +34,12 @@ struct lbm_handle {
     double *red = nullptr;
     void *scratch = nullptr;
     size_t scratch_bytes = 0;
+    // field transfers (lbm_read_fields / lbm_write_fields): a copy stream and
+    // per-half events, so that the copy of one field overlaps the conversion
+    // kernel of the next (two scratch halves)
+    cudaStream_t xstream = nullptr;
+    cudaEvent_t xe_copied[2] = {nullptr, nullptr};
+    cudaEvent_t xe_converted[2] = {nullptr, nullptr};
     float tau = 0, omega = 0, t_omega = 0, omega_d2 = 0;
     int64_t t = 0;
     lbm::Launcher launcher;
