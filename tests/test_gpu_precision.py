@@ -6,8 +6,8 @@ relative; over a run the rounding acts like noise that the collision only
 partly damps: FP16 stays within ~1% of the FP32 path, BF16 drifts by 10-30%
 (its 8-bit significand is too coarse for these moments).  The
 bounds below are stated per moment for D3Q19 128^3, Re = 1000, 2000 steps;
-tests/precision_report.py prints the full table (also against the FP64
-oracle)."""
+test_storage_formats_against_fp64_oracle bounds every format's error against
+the FP64 oracle after 1000 steps."""
 import numpy as np
 import pytest
 
