@@ -35,7 +35,7 @@ EXPORTS = ("lbm_config_default", "lbm_create", "lbm_destroy", "lbm_init_regions"
            "lbm_batch_autotune", "lbm_batch_get_info", "lbm_batch_configure", "lbm_cut_plane",
            "lbm_vts_write", "lbm_perturb_velocity", "lbm_filter_2to1", "lbm_trainer_create", "lbm_trainer_destroy",
            "lbm_trainer_add", "lbm_trainer_samples", "lbm_trainer_fit", "lbm_trainer_gradient", "lbm_mlp_infer",
-           "lbm_closure_set", "lbm_closure_dtau", "lbm_closure_refresh",
+           "lbm_closure_set", "lbm_closure_dtau", "lbm_closure_refresh", "lbm_closure_fused",
            "lbm_selftest_wait_timeout", "lbm_field_statistics")
 
 
@@ -171,6 +171,7 @@ def lib() -> ctypes.CDLL:
         L.lbm_closure_set.argtypes = [vp, ctypes.POINTER(MLP)]
         L.lbm_closure_dtau.argtypes = [vp, vp, sz]
         L.lbm_closure_refresh.argtypes = [vp, i32]
+        L.lbm_closure_fused.argtypes = [vp, i32]
         L.lbm_selftest_wait_timeout.argtypes = [i32, u64]
         L.lbm_field_statistics.argtypes = [i32, vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, i32, i32, vp, vp,
                                            vp]
@@ -184,7 +185,7 @@ def lib() -> ctypes.CDLL:
                      "lbm_cut_plane", "lbm_vts_write", "lbm_perturb_velocity", "lbm_filter_2to1",
                      "lbm_trainer_create", "lbm_trainer_destroy", "lbm_trainer_add", "lbm_trainer_samples",
                      "lbm_trainer_fit", "lbm_trainer_gradient", "lbm_mlp_infer", "lbm_closure_set",
-                     "lbm_closure_dtau", "lbm_closure_refresh", "lbm_selftest_wait_timeout",
+                     "lbm_closure_dtau", "lbm_closure_refresh", "lbm_closure_fused", "lbm_selftest_wait_timeout",
                      "lbm_field_statistics"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L

@@ -460,6 +460,27 @@ bool pick_closure(int Q, int tx, int ty, int stages, int npb, void *&fn, size_t 
     return false;
 }
 
+// The closure kernel with the network fused in, for a handle's kernel shape
+// (tiles of 128 or 256 threads); false: the shape has none.
+bool pick_closure_fused(int Q, int tx, int ty, int stages, int npb, void *&fn, size_t &smem)
+{
+#define LBM_FUSED_SHAPE(QQ, TXX, MINB)                                                                        \
+    if (Q == QQ && tx == TXX && ty == 8 && stages == 2 && npb == 1) {                                       \
+        fn = reinterpret_cast<void *>(&lbm::closure_fused_kernel<QQ, TXX, 8, 2, 1, MINB>);                   \
+        smem = lbm::FusedLayout<QQ, TXX, 8, 2, 1>::bytes;                                                   \
+        return true;                                                                                        \
+    }
+    LBM_FUSED_SHAPE(19, 32, 2)
+    LBM_FUSED_SHAPE(19, 16, 4)
+    LBM_FUSED_SHAPE(27, 32, 2)
+    LBM_FUSED_SHAPE(27, 16, 4)
+#undef LBM_FUSED_SHAPE
+    return false;
+}
+// shared memory of the fused shapes against the CTAs per SM their launch bounds assume
+static_assert(2 * (lbm::FusedLayout<27, 32, 8, 2, 1>::bytes + 1024) <= 228 * 1024, "fused 32x8: 2 CTAs per SM");
+static_assert(4 * (lbm::FusedLayout<27, 16, 8, 2, 1>::bytes + 1024) <= 228 * 1024, "fused 16x8: 4 CTAs per SM");
+
 }  // namespace
 
 // ------------------------------------------------------------ trainer
@@ -482,12 +503,59 @@ namespace lbm {
 // the tensor cores, then the closure step kernel.
 lbm_status closure_step(lbm_handle *h)
 {
+    void *ffn = nullptr;
+    size_t fsmem = 0;
+    if (h->closure_fused && h->closure_every == 1 &&
+        pick_closure_fused(h->Q, h->launcher.tx, h->launcher.ty, h->launcher.stages, h->launcher.pop_buffers, ffn,
+                           fsmem)) {
+        // the network inside the step kernel: no dtau array, one launch
+        struct Known {
+            const void *fn;
+            int device;
+        };
+        static std::mutex mu;
+        static std::vector<Known> known;
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            bool seen = false;
+            for (const Known &k : known)
+                seen |= (k.fn == ffn && k.device == h->cfg.device);
+            if (!seen) {
+                LBM_CUDA_RETURN(cudaFuncSetAttribute(ffn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(fsmem)));
+                known.push_back({ffn, h->cfg.device});
+            }
+        }
+        StepParams<float, float> p{};
+        const int nxt = h->cur ^ 1;
+        p.out = static_cast<float *>(h->m[nxt]);
+        p.nx = int(h->cfg.nx);
+        p.ny = int(h->cfg.ny);
+        p.nz = int(h->cfg.nz);
+        p.zc = h->zc;
+        p.rx = Relax{h->omega, h->t_omega, h->omega_d2, h->tau, h->cfg.u_inf};
+        p.fault = h->err;
+        p.timeout_ns = 2000000000ull;
+        MlpDevice net = *h->mlp;
+        const dim3 block(h->launcher.tx, h->launcher.ty);
+        const dim3 grid(unsigned((h->cfg.nx + h->launcher.tx - 1) / h->launcher.tx),
+                        unsigned((h->cfg.ny + h->launcher.ty - 1) / h->launcher.ty),
+                        unsigned((h->cfg.nz + h->zc - 1) / h->zc));
+        void *args[] = {&h->tmap[h->cur], &p, &net};
+        LBM_CUDA_RETURN(cudaLaunchKernel(ffn, grid, block, args, fsmem, h->stream));
+        h->closure_steps++;
+        h->dtau_current = false;
+        h->cur = nxt;
+        h->t += 1;
+        h->launches += 1;
+        return LBM_OK;
+    }
     if (h->closure_steps++ % uint64_t(h->closure_every) == 0) {
         lbm_status s = launch_infer(static_cast<const float *>(h->m[h->cur]), h->N, *h->mlp, h->dtau,
                                     &h->err->flags, true, false, h->stream, h->cfg.device);
         if (s != LBM_OK)
             return s;
         h->launches += 1;
+        h->dtau_current = true;
     }
     void *fn = nullptr;
     size_t smem = 0;
@@ -959,6 +1027,14 @@ lbm_status lbm_closure_set(lbm_handle *h, const lbm_mlp *net)
     return LBM_OK;
 }
 
+lbm_status lbm_closure_fused(lbm_handle *h, int32_t on)
+{
+    if (!h)
+        return fail(LBM_ERR_ARG, "lbm_closure_fused: null handle");
+    h->closure_fused = on != 0;
+    return LBM_OK;
+}
+
 lbm_status lbm_closure_refresh(lbm_handle *h, int32_t every)
 {
     if (!h || every < 1)
@@ -977,6 +1053,17 @@ lbm_status lbm_closure_dtau(lbm_handle *h, float *host, size_t count)
     if (count != h->N)
         return fail(LBM_ERR_ARG, "lbm_closure_dtau: count must be the node count");
     LBM_CUDA_RETURN(cudaSetDevice(h->cfg.device));
+    if (!h->dtau_current) {
+        // the last step evaluated the network inside the step kernel: the
+        // same network on that step's input state (the other moment buffer)
+        // gives its dtau, bit for bit
+        lbm_status s = launch_infer(static_cast<const float *>(h->m[h->cur ^ 1]), h->N, *h->mlp, h->dtau,
+                                    &h->err->flags, true, false, h->stream, h->cfg.device);
+        if (s != LBM_OK)
+            return s;
+        h->launches += 1;
+        h->dtau_current = true;
+    }
     LBM_CUDA_RETURN(cudaMemcpyAsync(host, h->dtau, count * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
     LBM_CUDA_RETURN(cudaStreamSynchronize(h->stream));
     return LBM_OK;

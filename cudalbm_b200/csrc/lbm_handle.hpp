@@ -56,6 +56,8 @@ struct lbm_handle {
     cudaGraphExec_t steps_graph = nullptr;  // kGraphSteps plain steps from buffer 0 (see lbm_step)
     int closure_every = 1;             // recompute dtau every this many steps
     uint64_t closure_steps = 0;        // closure steps taken since lbm_closure_set
+    bool closure_fused = true;         // evaluate the network inside the step kernel (when every == 1)
+    bool dtau_current = true;          // dtau[] holds the last closure step's values
 };
 
 namespace lbm {

@@ -33,7 +33,7 @@
 
 #include <cstdint>
 
-#include "lbm_step.cuh"
+#include "lbm_ptx.cuh"
 
 namespace lbm {
 
@@ -278,6 +278,144 @@ __device__ __forceinline__ bool mbar_wait_sleep_bounded(uint64_t *bar, unsigned 
         if (global_ns() - t0 > limit_ns)
             return false;
     }
+}
+
+// ---------------------------------------------- network fused into a step
+// The closure step kernel evaluates the network for the nodes of every plane
+// it receives, one M = 128 tile per group of four warps (128 threads), with
+// the same arithmetic as mlp_infer_kernel (so the same dtau, bit for bit):
+//   plane p received:  each thread writes its node's standardised features
+//                      (layer-1 operand row); after the CTA barrier the
+//                      group's leader issues layer 1 (K = 16);
+//   update of plane p-1: the group reads layer 2 of plane p-1 (issued one
+//                      plane earlier) and derives the nodes' dtau;
+//   after the update:  layer 1 of plane p is read back, biased, GELU'd and
+//                      written as the layer-2 operand; after a group barrier
+//                      the leader issues layer 2 (K = 32, two MMAs).
+// The tensor-core latency hides behind the plane's reconstruction and
+// update.  Layer 1 and layer 2 have separate operands and accumulators, so no
+// step waits for an MMA other than the one whose result it reads.
+struct FusedMlpSmem {
+    static constexpr int W1 = 0;                                     // 32 x 16 FP16 (shared by the groups)
+    static constexpr int W2 = W1 + kMlpHidden * kMlpIn * 2;          // 32 x 32 FP16
+    static constexpr int GROUP0 = W2 + kMlpHidden * kMlpHidden * 2;  // first group's operands
+    static constexpr int A1 = 0;                                     // 128 x 16 FP16 (group-relative)
+    static constexpr int A2 = A1 + 128 * kMlpIn * 2;                 // 128 x 32 FP16
+    static constexpr int GROUP_BYTES = A2 + 128 * kMlpHidden * 2;
+    template <int NG>
+    struct Of {
+        static constexpr int BARS = GROUP0 + NG * GROUP_BYTES;  // two mbarriers per group
+        static constexpr int TMEM = BARS + NG * 16;             // allocated tensor-memory address
+        static constexpr int BYTES = TMEM + 16;
+        static constexpr uint32_t COLS = NG == 1 ? 64 : 128;    // 64 columns per group, power of two
+    };
+    static constexpr uint32_t LBO_W = (kMlpHidden / 8) * 128, LBO_A = (128 / 8) * 128, SBO = 128;
+};
+static_assert(FusedMlpSmem::W2 % 128 == 0 && FusedMlpSmem::GROUP0 % 128 == 0 && FusedMlpSmem::A2 % 128 == 0 &&
+                  FusedMlpSmem::GROUP_BYTES % 128 == 0,
+              "operand alignment");
+
+// Per-thread view of its group's network state.
+struct FusedMlp {
+    __half *w1, *w2;        // shared operands
+    __half *a1, *a2;        // this group's operands
+    uint64_t *bar1, *bar2;  // this group's MMA-completion barriers
+    uint32_t tm1, tm2;      // this warp's lanes of the group's layer-1 / layer-2 accumulators
+    uint32_t t1_issue, t2_issue;  // the accumulators' base addresses (for the MMA)
+    int row;                // this thread's row of the group's tile
+    int group;              // group index (named barrier group + 1)
+    bool leader;            // issues the group's MMAs
+    unsigned ph1, ph2;      // parities the next waits expect
+    bool in_prev, in_cur;   // features in range: node updated next / node of this plane
+};
+
+// Layer-1 operand row from a node's stored moments; returns whether every
+// raw feature lies in the training range.
+__device__ __forceinline__ bool fused_features(FusedMlp &f, const MlpDevice &net, const float *m_stored)
+{
+    float x[kMlpIn];
+    node_features(m_stored, net.r_ii, net.r_ij, x);
+    const bool inside = in_range(x, net);
+#pragma unroll
+    for (int c = 0; c < kMlpIn / 8; c++) {
+        uint32_t p[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            p[j] = pack_f16x2_sat(fmaf(x[8 * c + 2 * j], net.in_scale[8 * c + 2 * j], net.in_shift[8 * c + 2 * j]),
+                                  fmaf(x[8 * c + 2 * j + 1], net.in_scale[8 * c + 2 * j + 1],
+                                       net.in_shift[8 * c + 2 * j + 1]));
+        store_chunk_f16(f.a1, f.row, 8 * c, 128, p[0], p[1], p[2], p[3]);
+    }
+    return inside;
+}
+
+// Layer 1 (16 -> 32) of the group's tile, by its leader, after the CTA barrier
+// that follows the operand writes (each writer fenced them for the async proxy).
+__device__ __forceinline__ void fused_issue_layer1(const FusedMlp &f)
+{
+    constexpr uint32_t idesc = umma_idesc_f16_f32<128, kMlpHidden>();
+    tc_fence_after();
+    umma_f16_if(f.leader, f.t1_issue, umma_desc(f.a1, FusedMlpSmem::LBO_A, FusedMlpSmem::SBO),
+                umma_desc(f.w1, FusedMlpSmem::LBO_W, FusedMlpSmem::SBO), idesc, false);
+    umma_commit_if(f.leader, f.bar1);
+}
+
+// Layer 1's accumulators -> bias, GELU -> layer-2 operand; group barrier;
+// layer 2 (32 -> 32) by the leader.  False when the wait for layer 1 gave up
+// (the MMA is then not issued; the caller aborts the CTA).
+__device__ __forceinline__ bool fused_layer2(FusedMlp &f, const MlpDevice &net, uint64_t timeout_ns)
+{
+    constexpr uint32_t idesc = umma_idesc_f16_f32<128, kMlpHidden>();
+    const bool ok = mbar_wait_sleep_bounded(f.bar1, f.ph1, timeout_ns);
+    f.ph1 ^= 1u;
+    tc_fence_after();
+    float z[kMlpHidden];
+    tmem_ld_32cols(f.tm1, z);
+#pragma unroll
+    for (int c = 0; c < kMlpHidden / 8; c++) {
+        uint32_t p[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int i = 8 * c + 2 * j;
+            p[j] = gelu_f16x2(pack_f16x2_sat(z[i] + net.b1[i], z[i + 1] + net.b1[i + 1]));
+        }
+        store_chunk_f16(f.a2, f.row, 8 * c, 128, p[0], p[1], p[2], p[3]);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncwarp();
+    asm volatile("bar.sync %0, 128;" ::"r"(f.group + 1) : "memory");
+    tc_fence_after();
+    const bool go = ok;  // a leader whose wait gave up issues nothing (the CTA then aborts)
+    for (int s = 0; s < kMlpHidden / 16; s++)
+        // one K-step of 16 spans two 8-wide K-chunks: 2 x LBO bytes = LBO halves
+        umma_f16_if(f.leader && go, f.t2_issue,
+                    umma_desc(f.a2 + s * FusedMlpSmem::LBO_A, FusedMlpSmem::LBO_A, FusedMlpSmem::SBO),
+                    umma_desc(f.w2 + s * FusedMlpSmem::LBO_W, FusedMlpSmem::LBO_W, FusedMlpSmem::SBO), idesc, s > 0);
+    umma_commit_if(f.leader && go, f.bar2);
+    return ok;
+}
+
+// Layer 2's accumulators -> bias, GELU, the 32 -> 1 layer -> dtau of the node
+// whose features were written one plane earlier (0 outside the training
+// range).  ok = false when the wait gave up.
+__device__ __forceinline__ float fused_dtau(FusedMlp &f, const MlpDevice &net, uint64_t timeout_ns, bool &ok)
+{
+    ok = mbar_wait_sleep_bounded(f.bar2, f.ph2, timeout_ns);
+    f.ph2 ^= 1u;
+    tc_fence_after();
+    float z[kMlpHidden];
+    tmem_ld_32cols(f.tm2, z);
+    tc_fence_before();
+    float y = net.b3;
+#pragma unroll
+    for (int i = 0; i < kMlpHidden; i += 2) {
+        const uint32_t g = gelu_f16x2(pack_f16x2_sat(z[i] + net.b2[i], z[i + 1] + net.b2[i + 1]));
+        const float2 h = __half22float2(*reinterpret_cast<const __half2 *>(&g));
+        y = fmaf(net.w3[i], h.x, y);
+        y = fmaf(net.w3[i + 1], h.y, y);
+    }
+    return f.in_prev ? fminf(fmaxf(net.out_scale * y, net.dtau_lo), net.dtau_hi) : 0.0f;
 }
 
 // ------------------------------------------------------- inference kernel

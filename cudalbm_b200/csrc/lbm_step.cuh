@@ -28,6 +28,8 @@
 #include <cuda_runtime.h>
 
 #include "lbm_core.cuh"
+#include "lbm_mlp.cuh"
+#include "lbm_ptx.cuh"
 
 namespace lbm {
 
@@ -64,90 +66,6 @@ struct Storage<__nv_bfloat16> {
     __device__ static float load(__nv_bfloat16 v, int) { return __bfloat162float(v); }
     __device__ static __nv_bfloat16 store(float v, int) { return __float2bfloat16_rn(v); }
 };
-
-// ------------------------------------------------------------------ PTX
-__device__ __forceinline__ unsigned smem_u32(const void *p)
-{
-    return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
-{
-    unsigned ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ uint64_t global_ns()
-{
-    uint64_t t;
-    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-    return t;
-}
-// Bounded wait: gives up after `limit_ns` and reports false.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity, uint64_t limit_ns)
-{
-    if (mbar_try_wait(bar, parity))
-        return true;
-    const uint64_t t0 = global_ns();
-    for (;;) {
-        for (int k = 0; k < 32; k++)
-            if (mbar_try_wait(bar, parity))
-                return true;
-        if (global_ns() - t0 > limit_ns)
-            return false;
-    }
-}
-// CTA-wide barrier.  Each warp first reconverges (__syncwarp), then the CTA
-// synchronises; a warp split across divergent paths when it reaches a CTA
-// barrier can be released only in part.
-__device__ __forceinline__ void cta_sync()
-{
-    __syncwarp();
-    asm volatile("barrier.sync 0;" ::: "memory");
-}
-
-// Thread-0 work as predicated instructions executed by the whole warp, so
-// that no branch splits warp 0 (every thread calls these; only those with
-// `pred` act).
-//   TMA issue: make earlier ordinary reads of the slot visible to the async
-//   proxy, arm the slot's mbarrier with the plane's bytes, start the copy.
-__device__ __forceinline__ void tma_issue_if(bool pred, void *dst, const CUtensorMap *map, int c0, int c1, int c2,
-                                             int c3, uint64_t *bar, unsigned bytes)
-{
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.u32 p, %8, 0;\n\t"
-        "@p fence.proxy.async.shared::cta;\n\t"
-        "@p mbarrier.arrive.expect_tx.shared::cta.b64 _, [%6], %7;\n\t"
-        "@p cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
-        "[%6];\n\t}" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar)), "r"(bytes),
-        "r"(unsigned(pred))
-        : "memory");
-}
-//   mbarrier set-up: count 1 (the arming thread), then publish the init.
-__device__ __forceinline__ void mbar_init_if(bool pred, uint64_t *bar)
-{
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.u32 p, %1, 0;\n\t"
-        "@p mbarrier.init.shared::cta.b64 [%0], 1;\n\t}" ::"r"(smem_u32(bar)),
-        "r"(unsigned(pred))
-        : "memory");
-}
-__device__ __forceinline__ void fence_mbar_init_if(bool pred)
-{
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.u32 p, %0, 0;\n\t"
-        "@p fence.mbarrier_init.release.cluster;\n\t}" ::"r"(unsigned(pred))
-        : "memory");
-}
 
 // ------------------------------------------------------------- params
 enum : unsigned { ERR_TMA_TIMEOUT = 1u };
@@ -242,6 +160,71 @@ struct ZGroups {
     static constexpr int NU = count_cz<Q>(1), NS = count_cz<Q>(0), ND = count_cz<Q>(-1);
 };
 
+// The x-y movers grouped by their in-plane step (cx, cy): group g holds the
+// directions with that step and cz = -1 (D), 0 (S), +1 (U), whichever the
+// lattice has (D3Q27: all three in every group; D3Q19: all three on the axes,
+// S alone on the diagonals).  In the population plane a group's (S, U) pair
+// is one float2 cell and its D one float cell, so a node stores and a
+// neighbour pulls a whole group with two shared-memory accesses.
+__host__ __device__ constexpr int group_cx(int g)
+{
+    constexpr int t[8] = {1, -1, 0, 0, 1, -1, 1, -1};
+    return t[g];
+}
+__host__ __device__ constexpr int group_cy(int g)
+{
+    constexpr int t[8] = {0, 0, 1, -1, 1, -1, -1, 1};
+    return t[g];
+}
+// direction q of lattice Q with step (cx, cy, cz), or -1
+template <int Q>
+__host__ __device__ constexpr int q_of_step(int cx, int cy, int cz)
+{
+    for (int q = 0; q < Q; q++)
+        if (cx_of(q) == cx && cy_of(q) == cy && cz_of(q) == cz)
+            return q;
+    return -1;
+}
+template <int Q>
+struct PopGroups {
+    static constexpr int NG = 8;
+    __host__ __device__ static constexpr int qD(int g) { return q_of_step<Q>(group_cx(g), group_cy(g), -1); }
+    __host__ __device__ static constexpr int qS(int g) { return q_of_step<Q>(group_cx(g), group_cy(g), 0); }
+    __host__ __device__ static constexpr int qU(int g) { return q_of_step<Q>(group_cx(g), group_cy(g), 1); }
+    // cells: groups with U first (float2 planes), then S-only groups (float
+    // planes), then the D planes; offsets in floats, in units of one plane
+    __host__ __device__ static constexpr int n_su()
+    {
+        int n = 0;
+        for (int g = 0; g < NG; g++)
+            n += qU(g) >= 0;
+        return n;
+    }
+    __host__ __device__ static constexpr int su_plane(int g)  // float2 plane index, groups with U
+    {
+        int n = 0;
+        for (int h = 0; h < g; h++)
+            n += qU(h) >= 0;
+        return n;
+    }
+    __host__ __device__ static constexpr int s_plane(int g)  // float plane index (after the float2 planes)
+    {
+        int n = 2 * n_su();
+        for (int h = 0; h < g; h++)
+            n += qU(h) < 0;
+        return n;
+    }
+    __host__ __device__ static constexpr int d_plane(int g)  // float plane index
+    {
+        int n = 2 * n_su();
+        for (int h = 0; h < NG; h++)
+            n += qU(h) < 0;
+        for (int h = 0; h < g; h++)
+            n += qD(h) >= 0;
+        return n;
+    }
+};
+
 // Compile-time loop helper: calls f(IC<i>{}) for i in [B, E).
 template <int V>
 struct IC {
@@ -256,8 +239,50 @@ __device__ __forceinline__ void static_for(F &&f)
     }
 }
 
+// Population-plane offsets (floats) of group g's cells at plane cell `cell`
+// (compile-time plane offsets).
+template <int Q, int TX, int TY, typename ST>
+struct PopCell {
+    using G = TileGeom<TX, TY, ST>;
+    using PG = PopGroups<Q>;
+    static constexpr int PLANE = G::PY * G::PX;
+    template <int g>
+    __device__ static int su(int cell)
+    {
+        constexpr int off = 2 * PG::su_plane(g) * PLANE;
+        return off + 2 * cell;
+    }
+    template <int g>
+    __device__ static int s(int cell)
+    {
+        constexpr int off = PG::s_plane(g) * PLANE;
+        return off + cell;
+    }
+    template <int g>
+    __device__ static int d(int cell)
+    {
+        constexpr int off = PG::d_plane(g) * PLANE;
+        return off + cell;
+    }
+};
+
+// Store the x-y movers of group g reconstructed at plane cell `cell`.
+template <int Q, int TX, int TY, typename ST, int g>
+__device__ __forceinline__ void store_group(float *pb, int cell, const RecPre &r, const float *m)
+{
+    using PG = PopGroups<Q>;
+    using C = PopCell<Q, TX, TY, ST>;
+    constexpr int qs = PG::qS(g), qu = PG::qU(g), qd = PG::qD(g);
+    if constexpr (qu >= 0)
+        *reinterpret_cast<float2 *>(pb + C::template su<g>(cell)) = make_float2(rec_q<Q, qs>(r, m), rec_q<Q, qu>(r, m));
+    else
+        pb[C::template s<g>(cell)] = rec_q<Q, qs>(r, m);
+    if constexpr (qd >= 0)
+        pb[C::template d<g>(cell)] = rec_q<Q, qd>(r, m);
+}
+
 // Reconstruct the x-y movers of ring node (rx, ry) that point into the tile
-// (those with the given sign of cx or cy) and store them into pop plane pb.
+// (the groups with the given sign of cx or cy) and store them into pop plane pb.
 template <int Q, int TX, int TY, int AXIS, int SIGN, typename ST>
 __device__ __forceinline__ void ring_pops(const ST *sm, float *pb, int rx, int ry)
 {
@@ -268,11 +293,12 @@ __device__ __forceinline__ void ring_pops(const ST *sm, float *pb, int rx, int r
         m[k] = Storage<ST>::load(sm[(k * G::RY + ry + 1) * G::TXP + rx + G::XPAD], k);
     m[0] = m[0] + 1.0f;
     const RecPre r = rec_pre<Q>(m);
-    static_for<0, XY<Q>::N>([&](auto s) {
-        constexpr int q = XY<Q>::q(decltype(s)::value);
-        constexpr int c = AXIS == 0 ? cx_of(q) : cy_of(q);
+    const int cell = (ry + 1) * G::PX + rx + 1;
+    static_for<0, PopGroups<Q>::NG>([&](auto gc) {
+        constexpr int g = decltype(gc)::value;
+        constexpr int c = AXIS == 0 ? group_cx(g) : group_cy(g);
         if constexpr (c == SIGN)
-            pb[(decltype(s)::value * G::PY + ry + 1) * G::PX + rx + 1] = rec_q<Q, q>(r, m);
+            store_group<Q, TX, TY, ST, g>(pb, cell, r, m);
     });
 }
 
@@ -325,15 +351,20 @@ static __device__ __noinline__ void record_fault(StepFault *f, unsigned flag, in
 // keep cycling from one item to the next; the mbarriers are initialised once
 // per CTA.  Returns false, uniformly across the CTA, when a TMA wait timed
 // out (the error flag is then set).
-template <int Q, int TX, int TY, int NSTAGE, bool FO, typename MeanT, bool MON, int NPB, typename ST, bool CL = false>
+//
+// CLM selects the relaxation: 0 the plain collision; 1 the learned closure
+// with dtau read per node from p.dtau; 2 the learned closure with the network
+// evaluated in this kernel (mlp: the thread's group state, net: the network;
+// see FusedMlp), the same dtau as mode 1 after mlp_infer_kernel, bit for bit.
+template <int Q, int TX, int TY, int NSTAGE, bool FO, typename MeanT, bool MON, int NPB, typename ST, int CLM = 0>
 __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepParams<MeanT, ST> &p, int bx, int by,
                                             int bz, unsigned g0, const CtaSmem<ST> &sh, int *s_abort, MonAcc &acc,
-                                            int item = -1, int mesh = -1)
+                                            int item = -1, int mesh = -1, FusedMlp *mlp = nullptr,
+                                            const MlpDevice *net = nullptr)
 {
     using G = TileGeom<TX, TY, ST>;
     using L = SmemLayout<Q, TX, TY, NSTAGE, NPB, ST>;
     using ZG = ZGroups<Q>;
-    constexpr int NXY = XY<Q>::N;
     uint64_t *const bars = sh.bars;
     ST *const stages = sh.stages;
     float *const pops = sh.pops;
@@ -348,6 +379,13 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
     const bool own = (x < p.nx) && (y < p.ny);
     const size_t N = size_t(p.nx) * p.ny * p.nz;
     const size_t plane = size_t(p.nx) * p.ny;
+    // node class bits of x and y (normalVector.cuh:321-334); z is added per plane
+    const unsigned type_xy = (x == 0 ? WEST : 0u) | (x == p.nx - 1 ? EAST : 0u) | (y == 0 ? SOUTH : 0u) |
+                             (y == p.ny - 1 ? NORTH : 0u);
+    using PG = PopGroups<Q>;
+    using C = PopCell<Q, TX, TY, ST>;
+    static_assert(PG::d_plane(PG::NG) == XY<Q>::N, "population-plane groups cover the x-y movers");
+    const int my_cell = (ty + 1) * G::PX + tx + 1;
 
     // first planes of the item (the slots were last read by ordinary loads)
 #pragma unroll
@@ -375,10 +413,12 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
         const size_t iu = size_t(zu) * plane + size_t(y) * p.nx + x;
         MeanT sm_old[6], km_old = MeanT(0);
         float dtau = 0.0f;
-        if constexpr (CL) {
+        if constexpr (CLM == 1) {
             if (upd)
                 dtau = p.dtau[iu];
         }
+        // the network runs for the planes this CTA updates (z0 .. z1-1)
+        const bool net_plane = (i >= 1) && (i <= nplanes - 2);
         if constexpr (FO) {
             if (upd) {
                 if (p.fo.SMean) {
@@ -403,18 +443,38 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
 #pragma unroll
             for (int k = 0; k < 10; k++)
                 m[k] = Storage<ST>::load(sm[(k * G::RY + ty + 1) * G::TXP + tx + G::XPAD], k);
+            if constexpr (CLM == 2) {
+                // this node's network features, from the stored values
+                if (net_plane) {
+                    mlp->in_cur = fused_features(*mlp, *net, m) && own;
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                }
+            }
             m[0] = m[0] + 1.0f;
             const RecPre r = rec_pre<Q>(m);
-            static_for<0, NXY>([&](auto s) {
-                constexpr int q = XY<Q>::q(decltype(s)::value);
-                pb[(decltype(s)::value * G::PY + ty + 1) * G::PX + tx + 1] = rec_q<Q, q>(r, m);
-            });
+            static_for<0, PG::NG>([&](auto gc) { store_group<Q, TX, TY, ST, decltype(gc)::value>(pb, my_cell, r, m); });
             U0[zslot<Q>(5)] = rec_q<Q, 5>(r, m);
             D0[zslot<Q>(6)] = rec_q<Q, 6>(r, m);
             S0[zslot<Q>(0)] = rec_q<Q, 0>(r, m);
         }
-        // ring nodes: only the directions that enter the tile
-        if (lin < G::RING) {
+        // ring nodes: only the directions that enter the tile.  With 32-wide
+        // tiles each side goes to one warp (the bottom and top rows, x = 0..31,
+        // to warps 0 and 1; the left and right columns, corners included, to
+        // warps 2 and 3), so no warp runs two sides one after the other.
+        if constexpr (TX == 32) {
+            const int w = lin >> 5, l = lin & 31;
+            if (w == 0) {
+                ring_pops<Q, TX, TY, 1, +1, ST>(sm, pb, l, -1);
+            } else if (w == 1) {
+                ring_pops<Q, TX, TY, 1, -1, ST>(sm, pb, l, TY);
+            } else if (w == 2) {
+                if (l < TY + 2)
+                    ring_pops<Q, TX, TY, 0, +1, ST>(sm, pb, -1, l - 1);
+            } else if (w == 3) {
+                if (l < TY + 2)
+                    ring_pops<Q, TX, TY, 0, -1, ST>(sm, pb, TX, l - 1);
+            }
+        } else if (lin < G::RING) {
             int r = lin;
             if (r < TX + 2) {
                 ring_pops<Q, TX, TY, 1, +1, ST>(sm, pb, r - 1, -1);
@@ -427,22 +487,41 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
                 ring_pops<Q, TX, TY, 0, -1, ST>(sm, pb, TX, r);
             }
         }
+        if constexpr (CLM == 2)
+            tc_fence_before();
         cta_sync();
         if (*s_abort)
             return false;
+        if constexpr (CLM == 2) {
+            if (net_plane)
+                fused_issue_layer1(*mlp);
+        }
 
         // the stage is consumed: refill it with plane i + NSTAGE
         tma_issue_if(lin == 0 && i + NSTAGE < nplanes, sm, tmap, x0 - G::XPAD, y0 - 1, pz + NSTAGE, 0, &bars[stage],
                      G::PLANE_BYTES);
 
         // pull the down-movers (cz = -1) that land on plane pz-1
-        static_for<0, NXY>([&](auto s) {
-            constexpr int q = XY<Q>::q(decltype(s)::value);
-            if constexpr (cz_of(q) == -1)
-                D0[zslot<Q>(q)] = pb[(decltype(s)::value * G::PY + ty + 1 - cy_of(q)) * G::PX + tx + 1 - cx_of(q)];
+        static_for<0, PG::NG>([&](auto gc) {
+            constexpr int g = decltype(gc)::value;
+            constexpr int qd = PG::qD(g);
+            constexpr int off = group_cy(g) * G::PX + group_cx(g);
+            if constexpr (qd >= 0) {
+                constexpr int sd = zslot<Q>(qd);
+                D0[sd] = pb[C::template d<g>(my_cell - off)];
+            }
         });
 
         if (i >= 2) {
+            if constexpr (CLM == 2) {
+                // dtau of the nodes updated now: layer 2 of the previous plane
+                bool ok = true;
+                dtau = fused_dtau(*mlp, *net, *s_abort ? 1000000ull : p.timeout_ns, ok);
+                if (!ok) {
+                    record_fault(p.fault, ERR_MMA_TIMEOUT, item, mesh, i, g0 + i, 2u, mlp->ph2 ^ 1u, mlp->bar2);
+                    *s_abort = 1;
+                }
+            }
             // update plane zu = pz - 1 from U(pz-2), S(pz-1), D(pz)
             float f[Q];
             static_for<0, Q>([&](auto qc) {
@@ -453,9 +532,9 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
                 if constexpr (c == -1) f[q] = D0[zslot<Q>(q)];
             });
             if (own) {
-                const unsigned type = node_type(x, y, zu, p.nx, p.ny, p.nz);
+                const unsigned type = type_xy | (zu == 0 ? BACK : 0u) | (zu == p.nz - 1 ? FRONT : 0u);
                 float m[10];
-                if constexpr (CL) {
+                if constexpr (CLM != 0) {
                     // interior nodes relax with tau0 + dtau; omega as the host
                     // derives it from tau, so dtau = 0 gives the plain bits
                     Relax r = p.rx;
@@ -513,13 +592,32 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
             }
         }
 
+        if constexpr (CLM == 2) {
+            // layer 1 of this plane -> layer-2 operand; layer 2 issued
+            if (net_plane) {
+                if (!fused_layer2(*mlp, *net, *s_abort ? 1000000ull : p.timeout_ns)) {
+                    record_fault(p.fault, ERR_MMA_TIMEOUT, item, mesh, i, g0 + i, 1u, mlp->ph1 ^ 1u, mlp->bar1);
+                    *s_abort = 1;
+                }
+                mlp->in_prev = mlp->in_cur;
+            }
+        }
+
         // keep this plane's same-plane and up-movers for the next updates
-        static_for<0, NXY>([&](auto s) {
-            constexpr int q = XY<Q>::q(decltype(s)::value);
-            if constexpr (cz_of(q) == 0)
-                S0[zslot<Q>(q)] = pb[(decltype(s)::value * G::PY + ty + 1 - cy_of(q)) * G::PX + tx + 1 - cx_of(q)];
-            if constexpr (cz_of(q) == 1)
-                U0[zslot<Q>(q)] = pb[(decltype(s)::value * G::PY + ty + 1 - cy_of(q)) * G::PX + tx + 1 - cx_of(q)];
+        static_for<0, PG::NG>([&](auto gc) {
+            constexpr int g = decltype(gc)::value;
+            constexpr int off = group_cy(g) * G::PX + group_cx(g);
+            constexpr int qs = PG::qS(g), qu = PG::qU(g);
+            constexpr int ss = zslot<Q>(qs);
+            const int cell = my_cell - off;
+            if constexpr (qu >= 0) {
+                constexpr int su_slot = zslot<Q>(qu);
+                const float2 su = *reinterpret_cast<const float2 *>(pb + C::template su<g>(cell));
+                S0[ss] = su.x;
+                U0[su_slot] = su.y;
+            } else {
+                S0[ss] = pb[C::template s<g>(cell)];
+            }
         });
 #pragma unroll
         for (int k = 0; k < ZG::NU; k++) {
@@ -622,10 +720,108 @@ __global__ void __launch_bounds__(TX *TY, MINB)
     s_abort = 0;
     cta_sync();
     MonAcc acc;
-    march_chunk<Q, TX, TY, NSTAGE, false, float, false, NPB, float, true>(&tmap_in, p, blockIdx.x, blockIdx.y,
-                                                                          blockIdx.z, 0u, sh, &s_abort, acc);
+    march_chunk<Q, TX, TY, NSTAGE, false, float, false, NPB, float, 1>(&tmap_in, p, blockIdx.x, blockIdx.y,
+                                                                       blockIdx.z, 0u, sh, &s_abort, acc);
     if (s_abort && lin == 0)
         drain_after_abort<NSTAGE>(sh.bars);
+}
+
+// Shared-memory offset of the fused network's operands (after the step's
+// own layout, 128-byte aligned) and the total for a closure_fused_kernel CTA.
+template <int Q, int TX, int TY, int NSTAGE, int NPB>
+struct FusedLayout {
+    using L = SmemLayout<Q, TX, TY, NSTAGE, NPB, float>;
+    static constexpr int NG = TX * TY / 128;
+    static constexpr size_t mlp_off = (L::bytes + 127) / 128 * 128;
+    static constexpr size_t bytes = mlp_off + FusedMlpSmem::Of<NG>::BYTES;
+};
+
+// One step with the learned closure, the network evaluated in the kernel
+// (march_chunk mode 2): FP32 storage, no function objects; every interior
+// node relaxes with tau0 + dtau from the network on its moments at the start
+// of the step -- the result of mlp_infer_kernel followed by closure_kernel,
+// bit for bit, without the per-node dtau array.  Tiles of 128 or 256
+// threads (one or two network groups).
+template <int Q, int TX, int TY, int NSTAGE, int NPB, int MINB>
+__global__ void __launch_bounds__(TX *TY, MINB)
+    closure_fused_kernel(const __grid_constant__ CUtensorMap tmap_in, const StepParams<float, float> p,
+                         const __grid_constant__ MlpDevice net)
+{
+    constexpr int NT = TX * TY;
+    static_assert(NT % 128 == 0 && NT <= 256, "one or two groups of four warps");
+    using FL = FusedLayout<Q, TX, TY, NSTAGE, NPB>;
+    using MS = FusedMlpSmem;
+    using MG = FusedMlpSmem::Of<FL::NG>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ int s_abort;
+    const CtaSmem<float> sh = cta_smem<Q, TX, TY, NSTAGE, NPB, float>(smem);
+    unsigned char *ms = smem + FL::mlp_off;
+    const int lin = threadIdx.y * TX + threadIdx.x;
+    const int warp = lin >> 5, grp = lin >> 7;
+    {
+        // FP16 weights (already in the operand layout) into shared memory
+        const uint32_t *g = reinterpret_cast<const uint32_t *>(net.w1);
+        uint32_t *d = reinterpret_cast<uint32_t *>(ms + MS::W1);
+        constexpr int n4 = (MS::GROUP0 - MS::W1) / 4;
+        static_assert(sizeof(net.w1) + sizeof(net.w2) == MS::GROUP0 - MS::W1, "weights");
+        for (int k = lin; k < n4; k += NT)
+            d[k] = g[k];
+    }
+    uint64_t *mbars = reinterpret_cast<uint64_t *>(ms + MG::BARS);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(ms + MG::TMEM);
+#pragma unroll
+    for (int s = 0; s < NSTAGE; s++)
+        mbar_init_if(lin == 0, &sh.bars[s]);
+#pragma unroll
+    for (int b = 0; b < 2 * FL::NG; b++)
+        mbar_init_if(lin == 0, &mbars[b]);
+    fence_mbar_init_if(lin == 0);
+    s_abort = 0;
+    if (warp == 0)
+        tmem_alloc_warp(tslot, MG::COLS);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the weights, for the MMAs
+    tc_fence_before();
+    cta_sync();
+    tc_fence_after();
+    const uint32_t tbase = *tslot;
+    FusedMlp f;
+    f.w1 = reinterpret_cast<__half *>(ms + MS::W1);
+    f.w2 = reinterpret_cast<__half *>(ms + MS::W2);
+    f.a1 = reinterpret_cast<__half *>(ms + MS::GROUP0 + grp * MS::GROUP_BYTES + MS::A1);
+    f.a2 = reinterpret_cast<__half *>(ms + MS::GROUP0 + grp * MS::GROUP_BYTES + MS::A2);
+    f.bar1 = &mbars[2 * grp];
+    f.bar2 = &mbars[2 * grp + 1];
+    f.t1_issue = tbase + uint32_t(grp * 64);  // columns: layer 1 at +0, layer 2 at +32
+    f.t2_issue = f.t1_issue + 32u;
+    const uint32_t lanes = uint32_t((warp & 3) * 32) << 16;
+    f.tm1 = f.t1_issue + lanes;
+    f.tm2 = f.t2_issue + lanes;
+    f.row = lin & 127;
+    f.group = grp;
+    f.leader = (lin & 127) == 0;
+    f.ph1 = f.ph2 = 0u;
+    f.in_prev = f.in_cur = false;
+    MonAcc acc;
+    march_chunk<Q, TX, TY, NSTAGE, false, float, false, NPB, float, 2>(&tmap_in, p, blockIdx.x, blockIdx.y,
+                                                                       blockIdx.z, 0u, sh, &s_abort, acc, -1, -1,
+                                                                       &f, &net);
+    if (s_abort) {
+        if (lin == 0)
+            drain_after_abort<NSTAGE>(sh.bars);
+        if (f.leader) {
+            // MMAs possibly still in flight: a bounded chance to finish
+            // before their tensor memory is released
+            for (unsigned ph = 0; ph < 2; ph++) {
+                (void)mbar_wait_bounded(f.bar1, ph, 1000000ull);
+                (void)mbar_wait_bounded(f.bar2, ph, 1000000ull);
+            }
+        }
+    }
+    tc_fence_before();
+    cta_sync();
+    tc_fence_after();
+    if (warp == 0)
+        tmem_dealloc_warp(tbase, MG::COLS);
 }
 
 // ------------------------------------------------------------ batches

@@ -142,6 +142,11 @@ class Cavity:
         """Recompute the closure's dtau every `every` steps (1: every step)."""
         _lib.check(_lib.lib().lbm_closure_refresh(self._h, int(every)))
 
+    def closure_fused(self, on: bool = True) -> None:
+        """Evaluate the closure network inside the step kernel (True, the
+        default) or in a separate inference kernel (False); same results."""
+        _lib.check(_lib.lib().lbm_closure_fused(self._h, int(bool(on))))
+
     def closure_dtau(self) -> np.ndarray:
         nz, ny, nx = self.shape
         out = np.empty((nz, ny, nx), np.float32)

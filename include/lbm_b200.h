@@ -381,6 +381,15 @@ lbm_status lbm_closure_refresh(lbm_handle *h, int32_t every);
 /* The dtau field of the last closure step ([z][y][x], count = nodes). */
 lbm_status lbm_closure_dtau(lbm_handle *h, float *host, size_t count);
 
+/* Where the network runs when it is evaluated every step: on (the default)
+ * inside the step kernel -- one launch per step, no per-node dtau array in
+ * HBM -- or off: a separate inference kernel writes dtau and the step kernel
+ * reads it.  Both give the same bits.  Kernel shapes without a fused variant
+ * (8-wide tiles) and lbm_closure_refresh intervals above 1 use the separate
+ * kernels.  Replaces: nothing in the reference (no closure); the collision it
+ * modifies is src/collision/secondOrder.cuh:93-105. */
+lbm_status lbm_closure_fused(lbm_handle *h, int32_t on);
+
 /* Self-test of the device-side failure path: a kernel waits with the step
  * kernels' bounded wait on an mbarrier that nothing arrives on; after
  * timeout_ns the wait gives up, records where, and the call returns

@@ -189,3 +189,31 @@ def test_closure_range_must_keep_the_viscosity_positive():
             c.set_closure(net)
         net.dtau_lo = 0.5 - tau + 1e-3
         c.set_closure(net)
+
+
+@pytest.mark.parametrize("q", [19, 27])
+@pytest.mark.parametrize("nx", [32, 16], ids=["tile32", "tile16"])
+def test_fused_network_equals_separate_kernels(samples, q, nx):
+    """The closure step with the network inside the step kernel (tcgen05
+    MMAs per plane, no dtau array) gives the bits of the separate inference
+    kernel followed by the closure step kernel: moments after several steps
+    and the dtau field of the last step."""
+    _, feats, targ, _, _ = samples
+    net = random_net(feats, targ, seed=11, scale=0.5)
+    shape = (nx, 16, 24)
+    with Cavity(q, *shape, 300.0, 0.05) as a, Cavity(q, *shape, 300.0, 0.05) as b:
+        for c in (a, b):
+            c.init_regions()
+            c.set_closure(net)
+        b.closure_fused(False)
+        a.step(7)
+        b.step(7)
+        a.synchronize()
+        b.synchronize()
+        assert a.info()["tile_x"] == nx
+        # one launch per fused step, two per separate step
+        assert b.info()["kernel_launches"] - a.info()["kernel_launches"] == 7
+        da, db = a.closure_dtau(), b.closure_dtau()
+        assert np.count_nonzero(db) > 0  # the network changes tau somewhere
+        assert np.array_equal(bits(da), bits(db))
+        assert np.array_equal(bits(a.read()), bits(b.read()))
