@@ -634,6 +634,10 @@ lbm_status lbm_create(const lbm_config *cfg, lbm_handle **out)
         return fail(LBM_ERR_ARG, "mesh dimensions must be positive multiples of 8 (block::nx() * nxBlocks() == nx)");
     if (c.nx > (1 << 30) || c.ny > (1 << 30) || c.nz > (1 << 30))
         return fail(LBM_ERR_ARG, "mesh dimension too large");
+    // the step kernels address a node within a field with 32 bits (the FP32
+    // state of 2^32 nodes would take 343 GB, beyond one GPU)
+    if (uint64_t(c.nx) * uint64_t(c.ny) * uint64_t(c.nz) >= (uint64_t(1) << 32))
+        return fail(LBM_ERR_ARG, "mesh too large: at most 2^32 - 1 nodes");
     if (!(c.Re > 0.0f) || !std::isfinite(c.u_inf))
         return fail(LBM_ERR_ARG, "Re must be positive and u_inf finite");
     if (c.mean_bits != 32 && c.mean_bits != 64)

@@ -279,10 +279,13 @@ __device__ __forceinline__ void boundary_moments(const float *s, unsigned t, con
 
     {
         const float nB = static_cast<float>(__popc(t & 0x3Fu));
-        // U<alpha>: only the North wall moves (U_North = {u_inf, 0, 0})
-        mom[1] = ((t & NORTH) ? U : 0.0f) / nB;
-        mom[2] = 0.0f / nB;
-        mom[3] = 0.0f / nB;
+        // U<alpha>: only the North wall moves (U_North = {u_inf, 0, 0}); the
+        // mean over the node's nB walls.  A zero numerator gives +0 for every
+        // nB, so only the North lid divides (the zero quotients are written
+        // as such: a zero numerator sends the IEEE division to its slow path)
+        mom[1] = (t & NORTH) ? U / nB : 0.0f;
+        mom[2] = 0.0f;
+        mom[3] = 0.0f;
         mom[4] = mom[1] * mom[1];
     }
     mom[7] = 0.0f;
@@ -518,7 +521,7 @@ __device__ __forceinline__ void node_update(float *f, unsigned type, const Relax
 // rounded quotient (P. Markstein, "Computation of elementary functions on the
 // IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990) as long as
 // nothing underflows or overflows: numerators must lie in [2^-64, 2^64) in
-// magnitude (zeros excluded); div_unsafe(x) >= 128 flags the others, which
+// magnitude or be +0; div_unsafe(x) >= 128 flags the others, which
 // div_exact() handles.  Both are checked against IEEE division for every
 // float numerator by tests/cuda/div_exhaustive.cu.
 __device__ __forceinline__ float div_by_recip(float x, float d, float r)
@@ -529,7 +532,10 @@ __device__ __forceinline__ float div_by_recip(float x, float d, float r)
 }
 __device__ __forceinline__ unsigned div_unsafe(float x)
 {
-    return ((__float_as_uint(x) >> 23) & 0xffu) - 63u;  // >= 128 when outside the window
+    // >= 128 when outside the window; +0 (bit pattern 0) counts as inside:
+    // div_by_recip returns +0 for it, the correctly rounded +0 / d
+    const unsigned b = __float_as_uint(x);
+    return b ? ((b >> 23) & 0xffu) - 63u : 0u;
 }
 
 // x / d rounded to nearest-even for any float x and d in [1, 2^40) with
@@ -612,7 +618,10 @@ __device__ __forceinline__ void strain_rate(const float *m, const StrainDiv &sd,
 }
 __device__ __forceinline__ float kinetic(float u, float v, float w)
 {
-    return sqrtf((u * u) + (v * v) + (w * w)) * 0.5f;
+    // a node at rest (+0, the sum of squares is never -0) skips the square
+    // root: sqrtf(+0) * 0.5 = +0, and a zero argument takes sqrtf's slow path
+    const float s = (u * u) + (v * v) + (w * w);
+    return s == 0.0f ? 0.0f : sqrtf(s) * 0.5f;
 }
 template <typename T>
 __device__ __forceinline__ T time_average(T mean, T f, T inv)

@@ -378,7 +378,8 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
     const int x = x0 + tx, y = y0 + ty;
     const bool own = (x < p.nx) && (y < p.ny);
     const size_t N = size_t(p.nx) * p.ny * p.nz;
-    const size_t plane = size_t(p.nx) * p.ny;
+    const uint32_t plane32 = uint32_t(p.nx) * uint32_t(p.ny);
+    const uint32_t row32 = uint32_t(y) * uint32_t(p.nx) + uint32_t(x);
     // node class bits of x and y (normalVector.cuh:321-334); z is added per plane
     const unsigned type_xy = (x == 0 ? WEST : 0u) | (x == p.nx - 1 ? EAST : 0u) | (y == 0 ? SOUTH : 0u) |
                              (y == p.ny - 1 ? NORTH : 0u);
@@ -395,10 +396,14 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
                      0, &bars[slot], G::PLANE_BYTES);
     }
 
-    // populations held in registers between planes
-    float U2[ZG::NU], U1[ZG::NU], S1[ZG::NS];  // U(p-2), U(p-1), S(p-1)
+    // Populations held in registers between planes: the up-movers of the
+    // two previous planes (UA for even i, UB for odd i) and the same-plane
+    // movers of the previous plane (S1).  The iteration for plane i reads
+    // U(i-2) from its set and S(i-1) in the update, then overwrites both
+    // with U(i) and S(i): no register moves, the loop runs two planes per trip.
+    float UA[ZG::NU], UB[ZG::NU], S1[ZG::NS];
 
-    for (int i = 0; i < nplanes; i++) {
+    auto plane_step = [&](const int i, float(&U2)[ZG::NU]) -> bool {
         const int pz = z0 - 1 + i;  // plane being received
         const unsigned g = g0 + i;
         const int stage = g % NSTAGE;
@@ -410,7 +415,10 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
         // loaded early so the latency hides behind the reconstruction
         const int zu = pz - 1;
         const bool upd = (i >= 2) && own;
-        const size_t iu = size_t(zu) * plane + size_t(y) * p.nx + x;
+        // node offset within a field (32 bits: lbm_create keeps every mesh
+        // below 2^32 nodes) against per-field base pointers, which are the
+        // same for the whole CTA
+        const uint32_t iu = uint32_t(zu) * plane32 + row32;
         MeanT sm_old[6], km_old = MeanT(0);
         float dtau = 0.0f;
         if constexpr (CLM == 1) {
@@ -424,7 +432,7 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
                 if (p.fo.SMean) {
 #pragma unroll
                     for (int c = 0; c < 6; c++)
-                        sm_old[c] = p.fo.SMean[c * N + iu];
+                        sm_old[c] = (p.fo.SMean + c * N)[iu];
                 }
                 if (p.fo.kMean)
                     km_old = p.fo.kMean[iu];
@@ -437,7 +445,8 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
         }
 
         // own node: reconstruct all directions
-        float U0[ZG::NU], S0[ZG::NS], D0[ZG::ND];
+        float D0[ZG::ND];
+        float own_up, own_rest;  // the pure-z up-mover and the rest population, kept for the next planes
         {
             float m[10];
 #pragma unroll
@@ -453,9 +462,9 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
             m[0] = m[0] + 1.0f;
             const RecPre r = rec_pre<Q>(m);
             static_for<0, PG::NG>([&](auto gc) { store_group<Q, TX, TY, ST, decltype(gc)::value>(pb, my_cell, r, m); });
-            U0[zslot<Q>(5)] = rec_q<Q, 5>(r, m);
+            own_up = rec_q<Q, 5>(r, m);
             D0[zslot<Q>(6)] = rec_q<Q, 6>(r, m);
-            S0[zslot<Q>(0)] = rec_q<Q, 0>(r, m);
+            own_rest = rec_q<Q, 0>(r, m);
         }
         // ring nodes: only the directions that enter the tile.  With 32-wide
         // tiles each side goes to one warp (the bottom and top rows, x = 0..31,
@@ -547,11 +556,10 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
                 } else {
                     node_update<Q>(f, type, p.rx, m);
                 }
-                ST *o = p.out + iu;
-                o[0] = Storage<ST>::store(m[0] - 1.0f, 0);
+                p.out[iu] = Storage<ST>::store(m[0] - 1.0f, 0);
 #pragma unroll
                 for (int k = 1; k < 10; k++)
-                    o[k * N] = Storage<ST>::store(m[k], k);
+                    (p.out + k * N)[iu] = Storage<ST>::store(m[k], k);
                 if constexpr (MON) {
                     acc.mass += double(m[0]);
                     acc.ke += double(m[0] * ((m[1] * m[1] + m[2] * m[2]) + m[3] * m[3]));
@@ -565,12 +573,12 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
                         if (p.fo.S) {
 #pragma unroll
                             for (int c = 0; c < 6; c++)
-                                p.fo.S[c * N + iu] = s6[c];
+                                (p.fo.S + c * N)[iu] = s6[c];
                         }
                         if (p.fo.SMean) {
 #pragma unroll
                             for (int c = 0; c < 6; c++)
-                                p.fo.SMean[c * N + iu] = time_average<MeanT>(sm_old[c], MeanT(s6[c]), p.fo.inv_count);
+                                (p.fo.SMean + c * N)[iu] = time_average<MeanT>(sm_old[c], MeanT(s6[c]), p.fo.inv_count);
                         }
                     }
                     if (p.fo.k || p.fo.kMean) {
@@ -584,7 +592,7 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
                         m[0] = m[0] - 1.0f;
 #pragma unroll
                         for (int c = 0; c < 10; c++) {
-                            MeanT *a = p.fo.momentsMean + c * N + iu;
+                            MeanT *a = p.fo.momentsMean + c * N + iu;  // (rare path)
                             *a = time_average<MeanT>(*a, MeanT(m[c]), p.fo.inv_count);
                         }
                     }
@@ -613,22 +621,24 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
             if constexpr (qu >= 0) {
                 constexpr int su_slot = zslot<Q>(qu);
                 const float2 su = *reinterpret_cast<const float2 *>(pb + C::template su<g>(cell));
-                S0[ss] = su.x;
-                U0[su_slot] = su.y;
+                S1[ss] = su.x;
+                U2[su_slot] = su.y;
             } else {
-                S0[ss] = pb[C::template s<g>(cell)];
+                S1[ss] = pb[C::template s<g>(cell)];
             }
         });
-#pragma unroll
-        for (int k = 0; k < ZG::NU; k++) {
-            U2[k] = U1[k];
-            U1[k] = U0[k];
-        }
-#pragma unroll
-        for (int k = 0; k < ZG::NS; k++)
-            S1[k] = S0[k];
+        U2[zslot<Q>(5)] = own_up;
+        S1[zslot<Q>(0)] = own_rest;
         if constexpr (NPB == 1)
             cta_sync();  // the single population plane is rewritten next iteration
+        return true;
+    };
+
+    for (int i = 0; i < nplanes; i += 2) {
+        if (!plane_step(i, UA))
+            return false;
+        if (i + 1 < nplanes && !plane_step(i + 1, UB))
+            return false;
     }
     return true;
 }

@@ -2,7 +2,8 @@
 // uniform strain-rate divisor) against IEEE division on the GPU: every float
 // bit pattern is used as the numerator (NaNs must give NaN).  Also counts,
 // per exponent of the numerator, where the unguarded Markstein step alone
-// would differ (that is what the guard in div_by_recip excludes).
+// would differ, and fails if any numerator the strain rate's guard
+// (div_unsafe) lets through to div_by_recip alone is among them.
 // Built and called by tests/test_gpu_division.py.
 #include <cuda_runtime.h>
 
@@ -27,8 +28,15 @@ __global__ void div_check(float d, float r, unsigned long long *bad, unsigned *f
             atomicMin(first, bits);
         }
         const float u = lbm::div_by_recip(x, d, r);
-        if (isfinite(x) && __float_as_uint(u) != __float_as_uint(b))
+        if (isfinite(x) && __float_as_uint(u) != __float_as_uint(b)) {
             atomicAdd(&hist[(bits >> 23) & 0xffu], 1ull);
+            // the strain rate's dispatch: a numerator div_unsafe() passes
+            // is divided by div_by_recip alone, so that must be exact too
+            if (lbm::div_unsafe(x) < 128u) {
+                n++;
+                atomicMin(first, bits);
+            }
+        }
     }
     if (n)
         atomicAdd(bad, n);

@@ -94,6 +94,10 @@ def test_abi_calls_that_need_no_gpu():
     cfg.nx, cfg.lattice = 16, 15
     assert L.lbm_create(ctypes.byref(cfg), ctypes.byref(h)) == 1
     assert L.lbm_create(None, ctypes.byref(h)) == 1
+    # node offsets within a field are 32-bit: 2^32 nodes or more are refused
+    cfg.lattice, cfg.nx, cfg.ny, cfg.nz = 19, 2048, 2048, 1024
+    assert L.lbm_create(ctypes.byref(cfg), ctypes.byref(h)) == 1
+    assert b"at most 2^32 - 1 nodes" in L.lbm_last_error()
 
 
 def test_batch_calls_that_need_no_gpu():
