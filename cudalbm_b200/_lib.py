@@ -61,7 +61,7 @@ class Info(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32), ("z_chunk", ctypes.c_int32),
                 ("stages", ctypes.c_int32), ("pop_buffers", ctypes.c_int32), ("ms_per_step", ctypes.c_double),
-                ("candidates", ctypes.c_int32), ("from_cache", ctypes.c_int32)]
+                ("candidates", ctypes.c_int32), ("from_cache", ctypes.c_int32), ("closure_fused", ctypes.c_int32)]
 
 
 class BatchInfo(ctypes.Structure):

@@ -1215,9 +1215,9 @@ void load_tune_file()
     TuneEntry e{};
     long long nx, ny, nz;
     unsigned fo;
-    while (std::fscanf(f, "%d %lld %lld %lld %u %d %d %d %d %d %d %lf", &e.key.Q, &nx, &ny, &nz, &fo, &e.key.mean_bits,
+    while (std::fscanf(f, "%d %lld %lld %lld %u %d %d %d %d %d %d %lf %d", &e.key.Q, &nx, &ny, &nz, &fo, &e.key.mean_bits,
                        &e.best.tile_x, &e.best.tile_y, &e.best.stages, &e.best.pop_buffers, &e.best.z_chunk,
-                       &e.best.ms_per_step) == 12) {
+                       &e.best.ms_per_step, &e.best.closure_fused) == 13) {
         e.key.nx = nx;
         e.key.ny = ny;
         e.key.nz = nz;
@@ -1235,9 +1235,9 @@ void save_tune_entry(const TuneEntry &e)
     FILE *f = std::fopen(path, "a");
     if (!f)
         return;
-    std::fprintf(f, "%d %lld %lld %lld %u %d %d %d %d %d %d %.6f\n", e.key.Q, (long long)e.key.nx, (long long)e.key.ny,
+    std::fprintf(f, "%d %lld %lld %lld %u %d %d %d %d %d %d %.6f %d\n", e.key.Q, (long long)e.key.nx, (long long)e.key.ny,
                  (long long)e.key.nz, e.key.fo, e.key.mean_bits, e.best.tile_x, e.best.tile_y, e.best.stages,
-                 e.best.pop_buffers, e.best.z_chunk, e.best.ms_per_step);
+                 e.best.pop_buffers, e.best.z_chunk, e.best.ms_per_step, e.best.closure_fused);
     std::fclose(f);
 }
 
@@ -1278,7 +1278,10 @@ lbm_status lbm_autotune(lbm_handle *h, int32_t trial_steps, lbm_tuning *out)
     LBM_CUDA(cudaSetDevice(h->cfg.device));
     if (trial_steps <= 0)
         trial_steps = 10;
-    const TuneKey key{h->Q, h->cfg.nx, h->cfg.ny, h->cfg.nz, h->cfg.function_objects, h->cfg.mean_bits};
+    // handles with a learned closure tune separately (closure kernel shapes)
+    const uint32_t kClosureKey = 0x100u;
+    const TuneKey key{h->Q, h->cfg.nx, h->cfg.ny, h->cfg.nz, h->cfg.function_objects | (h->closure ? kClosureKey : 0u),
+                      h->cfg.mean_bits};
     {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         load_tune_file();
@@ -1288,6 +1291,8 @@ lbm_status lbm_autotune(lbm_handle *h, int32_t trial_steps, lbm_tuning *out)
                                              e.best.z_chunk);
                 if (s != LBM_OK)
                     return s;
+                if (h->closure)
+                    h->closure_fused = e.best.closure_fused != 0;
                 if (out) {
                     *out = e.best;
                     out->from_cache = 1;
@@ -1319,9 +1324,11 @@ lbm_status lbm_autotune(lbm_handle *h, int32_t trial_steps, lbm_tuning *out)
     const int cur0 = h->cur;
     const int64_t t0 = h->t;
     const uint64_t launches0 = h->launches;
+    const uint64_t closure_steps0 = h->closure_steps;
     auto restore = [&]() {
         h->cur = cur0;
         h->t = t0;
+        h->closure_steps = closure_steps0;
         live[0].first = h->m[cur0];
         for (size_t i = 0; i < live.size(); i++)
             cudaMemcpyAsync(live[i].first, backup[i], live[i].second, cudaMemcpyDeviceToDevice, h->stream);
@@ -1377,6 +1384,30 @@ lbm_status lbm_autotune(lbm_handle *h, int32_t trial_steps, lbm_tuning *out)
     }
     lbm_status s = tried ? apply_variant(h, best.tile_x, best.tile_y, best.stages, best.pop_buffers, best.z_chunk)
                          : fail(LBM_ERR_STATE, "autotune: no kernel variant fits this mesh");
+    best.closure_fused = h->closure_fused ? 1 : 0;
+    if (s == LBM_OK && h->closure) {
+        // the learned closure's two evaluations on the chosen shape: the
+        // network inside the step kernel, or a separate inference kernel
+        double ms_mode[2] = {1e30, 1e30};
+        for (int fused = 0; fused < 2 && s == LBM_OK; fused++) {
+            h->closure_fused = fused != 0;
+            for (int w = 0; w < 2 && s == LBM_OK; w++)
+                s = md ? launch_step<double>(h) : launch_step<float>(h);
+            cudaEventRecord(h->ev0, h->stream);
+            for (int k = 0; k < trial_steps && s == LBM_OK; k++)
+                s = md ? launch_step<double>(h) : launch_step<float>(h);
+            cudaEventRecord(h->ev1, h->stream);
+            float ms = 0.0f;
+            if (s == LBM_OK && cudaEventSynchronize(h->ev1) == cudaSuccess &&
+                cudaEventElapsedTime(&ms, h->ev0, h->ev1) == cudaSuccess)
+                ms_mode[fused] = double(ms) / trial_steps;
+            restore();
+            tried++;
+        }
+        h->closure_fused = ms_mode[1] <= ms_mode[0];
+        best.closure_fused = h->closure_fused ? 1 : 0;
+        best.ms_per_step = std::min(ms_mode[0], ms_mode[1]);
+    }
     LBM_CUDA(cudaStreamSynchronize(h->stream));
     release();
     (void)launches0;

@@ -400,7 +400,8 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
     // two previous planes (UA for even i, UB for odd i) and the same-plane
     // movers of the previous plane (S1).  The iteration for plane i reads
     // U(i-2) from its set and S(i-1) in the update, then overwrites both
-    // with U(i) and S(i): no register moves, the loop runs two planes per trip.
+    // with U(i) and S(i): without function objects the loop runs two planes
+    // per trip and no population is moved between registers.
     float UA[ZG::NU], UB[ZG::NU], S1[ZG::NS];
 
     auto plane_step = [&](const int i, float(&U2)[ZG::NU]) -> bool {
@@ -634,11 +635,28 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
         return true;
     };
 
-    for (int i = 0; i < nplanes; i += 2) {
-        if (!plane_step(i, UA))
-            return false;
-        if (i + 1 < nplanes && !plane_step(i + 1, UB))
-            return false;
+    if constexpr (FO) {
+        // with the function objects the body is large: one plane per trip,
+        // the up-mover sets exchanged by register moves (two unrolled copies
+        // of this body measured slower: the autotuner then preferred the
+        // two-population-plane variant)
+        for (int i = 0; i < nplanes; i++) {
+            if (!plane_step(i, UA))
+                return false;
+#pragma unroll
+            for (int k = 0; k < ZG::NU; k++) {
+                const float t = UA[k];
+                UA[k] = UB[k];
+                UB[k] = t;
+            }
+        }
+    } else {
+        for (int i = 0; i < nplanes; i += 2) {
+            if (!plane_step(i, UA))
+                return false;
+            if (i + 1 < nplanes && !plane_step(i + 1, UB))
+                return false;
+        }
     }
     return true;
 }

@@ -172,6 +172,7 @@ typedef struct lbm_tuning {
     double ms_per_step;       /* measured device time per step of the chosen variant */
     int32_t candidates;       /* variants timed */
     int32_t from_cache;       /* 1 if taken from the cache without timing */
+    int32_t closure_fused;    /* with a learned closure: 1 if the network runs inside the step kernel */
 } lbm_tuning;
 
 /* Time every compiled kernel variant (tile shape, pipeline depth, population

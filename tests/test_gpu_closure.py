@@ -217,3 +217,23 @@ def test_fused_network_equals_separate_kernels(samples, q, nx):
         assert np.count_nonzero(db) > 0  # the network changes tau somewhere
         assert np.array_equal(bits(da), bits(db))
         assert np.array_equal(bits(a.read()), bits(b.read()))
+
+
+def test_autotune_picks_the_closure_evaluation_and_keeps_the_state(samples):
+    """With a closure set, the autotuner times the closure kernel shapes and
+    both evaluations of the network (inside the step kernel, or a separate
+    inference kernel), keeps the faster, and leaves the state as it was."""
+    _, feats, targ, _, _ = samples
+    net = random_net(feats, targ, seed=5, scale=0.5)
+    with Cavity(27, 32, 16, 24, 300.0, 0.05) as a, Cavity(27, 32, 16, 24, 300.0, 0.05) as b:
+        for c in (a, b):
+            c.init_regions()
+            c.set_closure(net)
+            c.step(3)
+        t = b.autotune(3)
+        assert t["closure_fused"] in (0, 1) and t["ms_per_step"] > 0
+        for c in (a, b):
+            c.step(5)
+            c.synchronize()
+        assert b.info()["step"] == 8
+        assert np.array_equal(bits(a.read()), bits(b.read()))
