@@ -1278,9 +1278,13 @@ lbm_status lbm_autotune(lbm_handle *h, int32_t trial_steps, lbm_tuning *out)
     LBM_CUDA(cudaSetDevice(h->cfg.device));
     if (trial_steps <= 0)
         trial_steps = 10;
-    // handles with a learned closure tune separately (closure kernel shapes)
-    const uint32_t kClosureKey = 0x100u;
-    const TuneKey key{h->Q, h->cfg.nx, h->cfg.ny, h->cfg.nz, h->cfg.function_objects | (h->closure ? kClosureKey : 0u),
+    // the size class: lattice, mesh, function objects, mean precision, and
+    // (in the high bits of the function-object word) the storage format and
+    // whether a learned closure is set -- each has its own kernel shapes
+    const uint32_t kClosureKey = 0x100u, kStorageShift = 9;
+    const TuneKey key{h->Q, h->cfg.nx, h->cfg.ny, h->cfg.nz,
+                      h->cfg.function_objects | (h->closure ? kClosureKey : 0u) |
+                          (uint32_t(h->storage) << kStorageShift),
                       h->cfg.mean_bits};
     {
         std::lock_guard<std::mutex> lock(g_tune_mu);

@@ -101,15 +101,21 @@ struct RecPre {
     float rhow[4];
 };
 
-template <int Q>
+// m[0] is rho; m[1..9] are the stored moments times SC = SCI, a power of two
+// (1 for the reference's values).  Every term of a population's bracket then
+// carries the factor SC and the weight carries 1/SC: each rounding is the
+// unscaled one scaled by an exact power of two, so the populations are the
+// same bits for every SC.
+template <int Q, int SCI = 1>
 __device__ __forceinline__ RecPre rec_pre(const float *m)
 {
+    constexpr float SC = float(SCI);
     RecPre r;
-    r.pics2 = 1.0f - Consts::cs2 * (m[4] + m[7] + m[9]);
-    r.rhow[0] = m[0] * weight<Q>(0);
-    r.rhow[1] = m[0] * weight<Q>(1);
-    r.rhow[2] = m[0] * weight<Q>(2);
-    r.rhow[3] = m[0] * weight<Q>(3);
+    r.pics2 = SC - Consts::cs2 * (m[4] + m[7] + m[9]);
+    r.rhow[0] = m[0] * (weight<Q>(0) / SC);
+    r.rhow[1] = m[0] * (weight<Q>(1) / SC);
+    r.rhow[2] = m[0] * (weight<Q>(2) / SC);
+    r.rhow[3] = m[0] * (weight<Q>(3) / SC);
     return r;
 }
 
@@ -476,32 +482,39 @@ __device__ __forceinline__ void boundary_moments(const float *s, unsigned t, con
 #undef LBM_MYZ_I
 }
 
-// velocitySet::scale followed by secondOrder::collide.
+// velocitySet::scale followed by secondOrder::collide.  With SC = SCI != 1 (a
+// power of two) the output comes out multiplied by SC: the scale factors take
+// SC and the quadratic terms' coefficients 1/SC, each product being the
+// unscaled one times SC exactly.
+template <int SCI = 1>
 __device__ __forceinline__ void scale_collide(float *m, const Relax &rx)
 {
-    m[1] = 3.0f * (m[1]);
-    m[2] = 3.0f * (m[2]);
-    m[3] = 3.0f * (m[3]);
-    m[4] = 4.5f * (m[4]);
-    m[5] = 9.0f * (m[5]);
-    m[6] = 9.0f * (m[6]);
-    m[7] = 4.5f * (m[7]);
-    m[8] = 9.0f * (m[8]);
-    m[9] = 4.5f * (m[9]);
+    constexpr float SC = float(SCI);
+    m[1] = (3.0f * SC) * (m[1]);
+    m[2] = (3.0f * SC) * (m[2]);
+    m[3] = (3.0f * SC) * (m[3]);
+    m[4] = (4.5f * SC) * (m[4]);
+    m[5] = (9.0f * SC) * (m[5]);
+    m[6] = (9.0f * SC) * (m[6]);
+    m[7] = (4.5f * SC) * (m[7]);
+    m[8] = (9.0f * SC) * (m[8]);
+    m[9] = (4.5f * SC) * (m[9]);
 
-    m[4] = rx.t_omega * m[4] + rx.omega_d2 * (m[1]) * (m[1]);
-    m[7] = rx.t_omega * m[7] + rx.omega_d2 * (m[2]) * (m[2]);
-    m[9] = rx.t_omega * m[9] + rx.omega_d2 * (m[3]) * (m[3]);
+    const float od2 = SC == 1.0f ? rx.omega_d2 : rx.omega_d2 * (1.0f / SC);
+    const float om = SC == 1.0f ? rx.omega : rx.omega * (1.0f / SC);
+    m[4] = rx.t_omega * m[4] + od2 * (m[1]) * (m[1]);
+    m[7] = rx.t_omega * m[7] + od2 * (m[2]) * (m[2]);
+    m[9] = rx.t_omega * m[9] + od2 * (m[3]) * (m[3]);
 
-    m[5] = rx.t_omega * m[5] + rx.omega * (m[1]) * (m[2]);
-    m[6] = rx.t_omega * m[6] + rx.omega * (m[1]) * (m[3]);
-    m[8] = rx.t_omega * m[8] + rx.omega * (m[2]) * (m[3]);
+    m[5] = rx.t_omega * m[5] + om * (m[1]) * (m[2]);
+    m[6] = rx.t_omega * m[6] + om * (m[1]) * (m[3]);
+    m[8] = rx.t_omega * m[8] + om * (m[2]) * (m[3]);
 }
 
 // Full node update from the streamed populations f[Q] (in direction order).
 // Returns the stored (post-collision) moments with rho still including rho0.
 // f is clobbered (unknown directions of boundary nodes are zeroed).
-template <int Q>
+template <int Q, int SCI = 1>
 __device__ __forceinline__ void node_update(float *f, unsigned type, const Relax &rx, float *m)
 {
     if (type)
@@ -512,7 +525,7 @@ __device__ __forceinline__ void node_update(float *f, unsigned type, const Relax
         boundary_moments<Q>(s, type, rx, m);
     else
         interior_moments(s, m);
-    scale_collide(m, rx);
+    scale_collide<SCI>(m, rx);
 }
 
 // ------------------------------------------------------- function objects

@@ -35,37 +35,74 @@ namespace lbm {
 
 // ------------------------------------------------------------ storage
 // How the 10 moment fields are held in HBM.  FP32 stores the reference's
-// values as they are.  The 16-bit formats store (value * scale[field]) with
-// power-of-two scales (exact to apply and undo) that bring typical cavity
-// magnitudes -- rho-1 ~ 1e-3, 3u ~ 0.1, 4.5 m_aa and 9 m_ab ~ 1e-2 -- near 1,
-// away from the fp16 subnormal range; arithmetic stays FP32.  XPAD is the
-// left padding of a TMA box so that its x start is 16-byte aligned.
+// values as they are.  FP16 stores value * SC with one power-of-two scale for
+// every field (exact to apply and undo), which lifts typical cavity magnitudes
+// -- rho-1 ~ 1e-3, 3u ~ 0.1, 4.5 m_aa and 9 m_ab ~ 1e-2 -- out of the FP16
+// subnormal range; BF16 has FP32's exponent range and stores the values as
+// they are.  Arithmetic stays FP32.  Because the scale is one power of two,
+// the step kernel never applies it: it reconstructs the populations from the
+// scaled moments with scaled constants and scales the collision's output
+// constants instead (see rec_pre / scale_collide), which rounds exactly as the
+// unscaled arithmetic would, so loading and storing a moment is one
+// conversion.  load/store (with the scale) serve the other kernels.  XPAD is
+// the left padding of a TMA box so that its x start is 16-byte aligned.
 template <typename ST>
 struct Storage;
 
 template <>
 struct Storage<float> {
     static constexpr int BYTES = 4, XPAD = 4;
-    __host__ __device__ static constexpr float scale(int) { return 1.0f; }
+    static constexpr int SCI = 1;
+    static constexpr float SC = float(SCI);
+    __host__ __device__ static constexpr float scale(int) { return SC; }
     __device__ static float load(float v, int) { return v; }
     __device__ static float store(float v, int) { return v; }
+    __device__ static float load_raw(float v) { return v; }
+    __device__ static float store_raw(float v) { return v; }
 };
 
 template <>
 struct Storage<__half> {
     static constexpr int BYTES = 2, XPAD = 8;
-    __host__ __device__ static constexpr float scale(int k) { return (k >= 1 && k <= 3) ? 8.0f : 64.0f; }
-    __device__ static float load(__half v, int k) { return __half2float(v) * (1.0f / scale(k)); }
-    __device__ static __half store(float v, int k) { return __float2half_rn(v * scale(k)); }
+    static constexpr int SCI = 64;
+    static constexpr float SC = float(SCI);
+    __host__ __device__ static constexpr float scale(int) { return SC; }
+    __device__ static float load(__half v, int) { return __half2float(v) * (1.0f / SC); }
+    __device__ static __half store(float v, int) { return __float2half_rn(v * SC); }
+    __device__ static float load_raw(__half v) { return __half2float(v); }
+    __device__ static __half store_raw(float v) { return __float2half_rn(v); }
 };
 
 template <>
 struct Storage<__nv_bfloat16> {
     static constexpr int BYTES = 2, XPAD = 8;
-    __host__ __device__ static constexpr float scale(int) { return 1.0f; }
+    static constexpr int SCI = 1;
+    static constexpr float SC = float(SCI);
+    __host__ __device__ static constexpr float scale(int) { return SC; }
     __device__ static float load(__nv_bfloat16 v, int) { return __bfloat162float(v); }
     __device__ static __nv_bfloat16 store(float v, int) { return __float2bfloat16_rn(v); }
+    __device__ static float load_raw(__nv_bfloat16 v) { return __bfloat162float(v); }
+    __device__ static __nv_bfloat16 store_raw(float v) { return __float2bfloat16_rn(v); }
 };
+
+// rho from a stored rho - 1 (scaled by SC): one rounding, as rho0 + value.
+template <typename ST>
+__device__ __forceinline__ float rho_of_stored(float v)
+{
+    if constexpr (Storage<ST>::SC == 1.0f)
+        return v + 1.0f;
+    else
+        return fmaf(v, 1.0f / Storage<ST>::SC, 1.0f);
+}
+// The stored value of rho: SC (rho - 1), rounded once.
+template <typename ST>
+__device__ __forceinline__ float stored_of_rho(float rho)
+{
+    if constexpr (Storage<ST>::SC == 1.0f)
+        return rho - 1.0f;
+    else
+        return fmaf(rho, Storage<ST>::SC, -Storage<ST>::SC);
+}
 
 // ------------------------------------------------------------- params
 enum : unsigned { ERR_TMA_TIMEOUT = 1u };
@@ -290,9 +327,9 @@ __device__ __forceinline__ void ring_pops(const ST *sm, float *pb, int rx, int r
     float m[10];
 #pragma unroll
     for (int k = 0; k < 10; k++)
-        m[k] = Storage<ST>::load(sm[(k * G::RY + ry + 1) * G::TXP + rx + G::XPAD], k);
-    m[0] = m[0] + 1.0f;
-    const RecPre r = rec_pre<Q>(m);
+        m[k] = Storage<ST>::load_raw(sm[(k * G::RY + ry + 1) * G::TXP + rx + G::XPAD]);
+    m[0] = rho_of_stored<ST>(m[0]);
+    const RecPre r = rec_pre<Q, Storage<ST>::SCI>(m);
     const int cell = (ry + 1) * G::PX + rx + 1;
     static_for<0, PopGroups<Q>::NG>([&](auto gc) {
         constexpr int g = decltype(gc)::value;
@@ -452,7 +489,7 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
             float m[10];
 #pragma unroll
             for (int k = 0; k < 10; k++)
-                m[k] = Storage<ST>::load(sm[(k * G::RY + ty + 1) * G::TXP + tx + G::XPAD], k);
+                m[k] = Storage<ST>::load_raw(sm[(k * G::RY + ty + 1) * G::TXP + tx + G::XPAD]);
             if constexpr (CLM == 2) {
                 // this node's network features, from the stored values
                 if (net_plane) {
@@ -460,8 +497,8 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
                     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 }
             }
-            m[0] = m[0] + 1.0f;
-            const RecPre r = rec_pre<Q>(m);
+            m[0] = rho_of_stored<ST>(m[0]);
+            const RecPre r = rec_pre<Q, Storage<ST>::SCI>(m);
             static_for<0, PG::NG>([&](auto gc) { store_group<Q, TX, TY, ST, decltype(gc)::value>(pb, my_cell, r, m); });
             own_up = rec_q<Q, 5>(r, m);
             D0[zslot<Q>(6)] = rec_q<Q, 6>(r, m);
@@ -555,12 +592,19 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
                     }
                     node_update<Q>(f, type, r, m);
                 } else {
-                    node_update<Q>(f, type, p.rx, m);
+                    node_update<Q, Storage<ST>::SCI>(f, type, p.rx, m);
                 }
-                p.out[iu] = Storage<ST>::store(m[0] - 1.0f, 0);
+                // m[1..9] come out of the collision scaled by SC, m[0] is rho
+                p.out[iu] = Storage<ST>::store_raw(stored_of_rho<ST>(m[0]));
 #pragma unroll
                 for (int k = 1; k < 10; k++)
-                    (p.out + k * N)[iu] = Storage<ST>::store(m[k], k);
+                    (p.out + k * N)[iu] = Storage<ST>::store_raw(m[k]);
+                if constexpr (Storage<ST>::SC != 1.0f && (MON || FO)) {
+                    // the monitor and the function objects take the moments unscaled
+#pragma unroll
+                    for (int k = 1; k < 10; k++)
+                        m[k] = m[k] * (1.0f / Storage<ST>::SC);
+                }
                 if constexpr (MON) {
                     acc.mass += double(m[0]);
                     acc.ke += double(m[0] * ((m[1] * m[1] + m[2] * m[2]) + m[3] * m[3]));

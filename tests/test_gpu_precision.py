@@ -126,3 +126,21 @@ def test_storage_formats_against_fp64_oracle(oracle_1000, storage):
     bmax, brel = ORACLE_BOUNDS[storage]
     assert np.all(mx <= bmax), (mx, bmax)
     assert np.all(rl <= brel), (rl, brel)
+
+
+def test_tuning_cache_separates_storage_formats():
+    """The autotuner's cache is keyed on the storage format too: tuning an
+    FP32 cavity and then a 16-bit one of the same mesh tunes each on its own
+    kernel shapes (a shape of one format may not exist in another)."""
+    shape = (64, 40, 24)  # a size class no other test tunes
+    with Cavity(19, *shape, 300.0, 0.05) as a:
+        a.init_regions()
+        ta = a.autotune(2)
+    for st in ("f16", "bf16"):
+        with Cavity(19, *shape, 300.0, 0.05, storage=st) as b:
+            b.init_regions()
+            tb = b.autotune(2)
+            assert tb["from_cache"] == 0 and tb["candidates"] >= 1
+            b.step(3)
+            b.synchronize()
+    assert ta["candidates"] >= 1
