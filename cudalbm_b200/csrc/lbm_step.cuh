@@ -679,11 +679,10 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
         return true;
     };
 
-    if constexpr (FO) {
-        // with the function objects the body is large: one plane per trip,
-        // the up-mover sets exchanged by register moves (two unrolled copies
-        // of this body measured slower: the autotuner then preferred the
-        // two-population-plane variant)
+    if constexpr (FO || CLM == 2) {
+        // with the function objects or the fused network the body is large:
+        // one plane per trip, the up-mover sets exchanged by register moves
+        // (two unrolled copies of these bodies measured slower)
         for (int i = 0; i < nplanes; i++) {
             if (!plane_step(i, UA))
                 return false;
