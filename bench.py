@@ -30,7 +30,8 @@ the slowest rank's time.
 
 --impl reference runs the reference's own solver, built from its sources into
 oracle/_ref (its only implementation is CUDA), on the same case, timing K steps
-after W from its per-step progress lines.
+from its progress lines (printed every K steps, the first timed one at the
+first multiple of K at or after W).
 """
 from __future__ import annotations
 
@@ -546,8 +547,10 @@ def run_closure(args, w):
 
 # ------------------------------------------------------- reference arm
 def reference_step_time(exe, spec, W, K, local):
-    """Seconds per step of the reference executable on one case, from its
-    per-step 'Time:' lines (K steps after W); (dt, clocks, error)."""
+    """Seconds per step of the reference executable on one case, from two of
+    its 'Time:' progress lines K steps apart, the first at the first multiple
+    of K at or after W (the case prints every K steps, so no per-step output
+    is timed); (dt, clocks, error)."""
     from cudalbm_b200 import casefiles
 
     with tempfile.TemporaryDirectory() as case:
@@ -581,6 +584,14 @@ def reference_step_time(exe, spec, W, K, local):
     return (stamps[W + K] - stamps[W]) / K, clocks, None
 
 
+def reference_case(spec_kw, W, K):
+    """Case settings for reference_step_time: progress lines every K steps,
+    timing from step W0 = the first multiple of K at or after W to W0 + K;
+    returns (spec keyword arguments, W0)."""
+    W0 = -(-W // K) * K
+    return dict(spec_kw, n_steps=W0 + K + 1, save_interval=W0 + K + 10, info_interval=K), W0
+
+
 def run_reference(args, w):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -600,9 +611,8 @@ def run_reference(args, w):
         per_edge, clocks = {}, None
         for e in sorted({c["nx"] for c in cavs}):
             c0 = next(c for c in cavs if c["nx"] == e)
-            spec = casefiles.CaseSpec(nx=e, ny=e, nz=e, Re=c0["Re"], u_inf=w["u"], n_steps=W + K + 1,
-                                      save_interval=W + K + 10, info_interval=1)
-            dt, clk, err = reference_step_time(exe, spec, W, K, local)
+            kw, W0 = reference_case(dict(nx=e, ny=e, nz=e, Re=c0["Re"], u_inf=w["u"]), W, K)
+            dt, clk, err = reference_step_time(exe, casefiles.CaseSpec(**kw), W0, K, local)
             if err:
                 return {"impl": "reference", "unavailable": err}
             per_edge[e] = dt
@@ -620,16 +630,16 @@ def run_reference(args, w):
             w = dict(w, n=(nx, ny, nz), Re=w["u"] * (nx - 1) / ((w["tau"] - 0.5) / 3.0))
         nx, ny, nz = w["n"]
         nodes = nx * ny * nz
-        spec = casefiles.CaseSpec(nx=nx, ny=ny, nz=nz, Re=w["Re"], u_inf=w["u"], n_steps=W + K + 1,
-                                  save_interval=W + K + 10, info_interval=1, function_objects=w["fo"])
-        dt, clocks, err = reference_step_time(exe, spec, W, K, local)
+        kw, W0 = reference_case(dict(nx=nx, ny=ny, nz=nz, Re=w["Re"], u_inf=w["u"], function_objects=w["fo"]), W, K)
+        dt, clocks, err = reference_step_time(exe, casefiles.CaseSpec(**kw), W0, K, local)
         if err:
             return {"impl": "reference", "unavailable": err}
         cfg = {"workload": w["desc"], "lattice": f"D3Q{w['lattice']}", "nx": nx, "ny": ny, "nz": nz,
                "Re": w["Re"], "u_lid": w["u"], "function_objects": list(w["fo"]), "parallelism": "1 GPU"}
         sample = (f"the reference's own executable (oracle/_ref/momentBasedD3Q{w['lattice']}, built from its "
-                  f"sources for sm_100a) on the B200 -- its only implementation is CUDA; {K} steps after {W}, timed "
-                  "by its per-step 'Time:' lines (wall clock, the reference synchronises the device every step)")
+                  f"sources for sm_100a) on the B200 -- its only implementation is CUDA; {K} steps after "
+                  f"{-(-W // K) * K} (the first multiple of K at or after W={W}), timed by two of its 'Time:' progress "
+                  "lines, printed every K steps (wall clock; the reference synchronises the device every step)")
     value = nodes / dt / 1e6
     return {
         "impl": "reference",
