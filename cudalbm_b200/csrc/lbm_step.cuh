@@ -441,7 +441,9 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
     // per trip and no population is moved between registers.
     float UA[ZG::NU], UB[ZG::NU], S1[ZG::NS];
 
-    auto plane_step = [&](const int i, float(&U2)[ZG::NU]) -> bool {
+    // U2 holds U(i-2) on entry; U(i) is written into Unew (which may be U2
+    // itself: the update has read U2 before the plane's up-movers are pulled)
+    auto plane_step = [&](const int i, float(&U2)[ZG::NU], float(&Unew)[ZG::NU]) -> bool {
         const int pz = z0 - 1 + i;  // plane being received
         const unsigned g = g0 + i;
         const int stage = g % NSTAGE;
@@ -667,12 +669,12 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
                 constexpr int su_slot = zslot<Q>(qu);
                 const float2 su = *reinterpret_cast<const float2 *>(pb + C::template su<g>(cell));
                 S1[ss] = su.x;
-                U2[su_slot] = su.y;
+                Unew[su_slot] = su.y;
             } else {
                 S1[ss] = pb[C::template s<g>(cell)];
             }
         });
-        U2[zslot<Q>(5)] = own_up;
+        Unew[zslot<Q>(5)] = own_up;
         S1[zslot<Q>(0)] = own_rest;
         if constexpr (NPB == 1)
             cta_sync();  // the single population plane is rewritten next iteration
@@ -681,23 +683,25 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
 
     if constexpr (FO || CLM == 2) {
         // with the function objects or the fused network the body is large:
-        // one plane per trip, the up-mover sets exchanged by register moves
+        // one plane per trip, the up-mover sets rotated by register moves
         // (two unrolled copies of these bodies measured slower)
+        // (UA: U(i-2), UB: U(i-1); the new set rotates in with two moves per
+        // direction)
         for (int i = 0; i < nplanes; i++) {
-            if (!plane_step(i, UA))
+            float U0[ZG::NU];
+            if (!plane_step(i, UA, U0))
                 return false;
 #pragma unroll
             for (int k = 0; k < ZG::NU; k++) {
-                const float t = UA[k];
                 UA[k] = UB[k];
-                UB[k] = t;
+                UB[k] = U0[k];
             }
         }
     } else {
         for (int i = 0; i < nplanes; i += 2) {
-            if (!plane_step(i, UA))
+            if (!plane_step(i, UA, UA))
                 return false;
-            if (i + 1 < nplanes && !plane_step(i + 1, UB))
+            if (i + 1 < nplanes && !plane_step(i + 1, UB, UB))
                 return false;
         }
     }

@@ -1,10 +1,12 @@
 """What the trained network gains over the method without it (GPU).
 
-A reduced closure study (cudalbm_b200/closure_study.py): D3Q27 cavity on a
-32^3 grid at the coarse relaxation time 0.5077 (Re 604), trained on eight
-perturbed 64^3 runs, shrink factor calibrated on a ninth, measured against the
-unperturbed 64^3 run box-filtered 2:1 (and sampled at the coarse nodes).
-Samples and training are deterministic, so the numbers below repeat.
+Reduced closure studies (cudalbm_b200/closure_study.py): D3Q27 cavity on a
+32^3 grid (Re 604; 5,000 coarse steps) and on a 64^3 grid (Re 1227; 10,000
+coarse steps, the largest that fits the test budget: about a minute) at the
+coarse relaxation time 0.5077, each trained on eight perturbed runs at twice
+the resolution, shrink factor calibrated on a ninth, measured against the
+unperturbed fine run box-filtered 2:1 (and sampled at the coarse nodes).
+Samples and training are deterministic, so the numbers repeat.
 """
 import json
 import os
@@ -16,9 +18,10 @@ from cudalbm_b200.closure_study import run_study
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module")
-def study():
-    r = run_study(nc=32, coarse_steps=5000, log=lambda s: None)
+@pytest.fixture(scope="module", params=[(32, 5000), (64, 10000)], ids=["32", "64"])
+def study(request):
+    nc, steps = request.param
+    r = run_study(nc=nc, coarse_steps=steps, log=lambda s: None)
     out = os.environ.get("LBM_B200_STUDY_JSON")
     if out:
         with open(out, "w") as fh:
