@@ -1341,7 +1341,8 @@ lbm_status lbm_autotune(lbm_handle *h, int32_t trial_steps, lbm_tuning *out)
     lbm_tuning best{};
     best.ms_per_step = 1e30;
     int tried = 0;
-    const int zcs[] = {2, 4, 8, 16, 32, 64};
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->cfg.device);
     for (const Variant &v : kVariants) {
         if (v.Q != h->Q || v.storage != h->storage || v.tx > h->cfg.nx || v.ty > h->cfg.ny)
             continue;
@@ -1351,6 +1352,28 @@ lbm_status lbm_autotune(lbm_handle *h, int32_t trial_steps, lbm_tuning *out)
         // (such a chunk re-reads two planes for every 2-4 it updates)
         const int64_t tiles = ((h->cfg.nx + v.tx - 1) / v.tx) * ((h->cfg.ny + v.ty - 1) / v.ty);
         const bool small = tiles * ((h->cfg.nz + 7) / 8) < 4 * 148 * 3;
+        // Candidates: powers of two, and chunk lengths whose grid is close to
+        // a whole number of waves of resident CTAs (k waves for k = 1..12):
+        // the last wave of a grid 9.2 waves long runs the GPU at a fifth of
+        // its CTA slots.  Chunks need not divide nz (the last is shorter).
+        std::vector<int> zcs = {2, 4, 8, 16, 32, 64};
+        {
+            Launcher l;
+            int per_sm = 0;
+            if (pick_launcher(h->Q, v.tx, v.ty, v.stages, v.npb, h->storage, h->cfg.function_objects != 0,
+                              h->cfg.mean_bits, l) &&
+                cudaFuncSetAttribute(l.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(l.smem)) == cudaSuccess &&
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, l.fn, v.tx * v.ty, l.smem) == cudaSuccess &&
+                per_sm > 0) {
+                const int64_t resident = int64_t(per_sm) * sms;
+                for (int64_t k = 1; k <= 12; k++) {
+                    const int64_t chunks = std::max<int64_t>(1, (k * resident + tiles / 2) / tiles);
+                    const int zc = int((h->cfg.nz + chunks - 1) / chunks);
+                    if (std::find(zcs.begin(), zcs.end(), zc) == zcs.end())
+                        zcs.push_back(zc);
+                }
+            }
+        }
         for (int zc : zcs) {
             if (zc > h->cfg.nz || (zc < 8 && !small))
                 continue;

@@ -11,6 +11,7 @@ Samples and training are deterministic, so the numbers repeat.
 import json
 import os
 
+import numpy as np
 import pytest
 
 from cudalbm_b200.closure_study import run_study
@@ -34,7 +35,8 @@ def test_network_learns_the_targets(study):
     assert t["samples"] > 100000
     assert t["loss_last"] < 0.5 * t["loss_first"]
     assert t["r2_held_out"] > 0.8
-    lo, hi = study["config"]["dtau_range"]
+    # the clamp bounds are float32 values (float32(0.05) > 0.05)
+    lo, hi = (float(np.float32(v)) for v in study["config"]["dtau_range"])
     assert lo <= study["dtau"]["mean"] <= hi and study["dtau"]["max"] <= hi
     assert study["dtau"]["nonzero_fraction"] > 0.0
 
