@@ -222,7 +222,7 @@ using lbm::Launcher;
 using lbm::Variant;
 using lbm::kVariants;
 
-bool pick_launcher(int Q, int tx, int ty, int stages, int npb, int storage, bool fo, int mean_bits, Launcher &out)
+bool pick_launcher(int Q, int tx, int ty, int stages, int npb, int storage, unsigned fo, int mean_bits, Launcher &out)
 {
     if (storage == 1)
         return lbm::pick_f16(Q, tx, ty, stages, npb, fo, mean_bits, out);
@@ -674,7 +674,7 @@ lbm_status lbm_create(const lbm_config *cfg, lbm_handle **out)
     if (c.tile_y) ty = c.tile_y;
     if (c.z_chunk) zc = c.z_chunk;
     if (c.stages) st = c.stages;
-    const bool fo = c.function_objects != 0;
+    const unsigned fo = c.function_objects;
     const int npb = c.pop_buffers ? c.pop_buffers : 1;
     if (h->storage && tx == 8)
         tx = 16;
@@ -1245,7 +1245,7 @@ void save_tune_entry(const TuneEntry &e)
 lbm_status apply_variant(lbm_handle *h, int tx, int ty, int stages, int npb, int zc)
 {
     Launcher l;
-    if (!pick_launcher(h->Q, tx, ty, stages, npb, h->storage, h->cfg.function_objects != 0, h->cfg.mean_bits, l))
+    if (!pick_launcher(h->Q, tx, ty, stages, npb, h->storage, h->cfg.function_objects, h->cfg.mean_bits, l))
         return fail(LBM_ERR_ARG, "unsupported tile configuration");
     for (void *fn : {l.fn, l.fn_mon})
         LBM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(l.smem)));
@@ -1360,7 +1360,7 @@ lbm_status lbm_autotune(lbm_handle *h, int32_t trial_steps, lbm_tuning *out)
         {
             Launcher l;
             int per_sm = 0;
-            if (pick_launcher(h->Q, v.tx, v.ty, v.stages, v.npb, h->storage, h->cfg.function_objects != 0,
+            if (pick_launcher(h->Q, v.tx, v.ty, v.stages, v.npb, h->storage, h->cfg.function_objects,
                               h->cfg.mean_bits, l) &&
                 cudaFuncSetAttribute(l.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(l.smem)) == cudaSuccess &&
                 cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, l.fn, v.tx * v.ty, l.smem) == cudaSuccess &&

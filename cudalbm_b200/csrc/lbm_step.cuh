@@ -393,7 +393,10 @@ static __device__ __noinline__ void record_fault(StepFault *f, unsigned flag, in
 // with dtau read per node from p.dtau; 2 the learned closure with the network
 // evaluated in this kernel (mlp: the thread's group state, net: the network;
 // see FusedMlp), the same dtau as mode 1 after mlp_infer_kernel, bit for bit.
-template <int Q, int TX, int TY, int NSTAGE, bool FO, typename MeanT, bool MON, int NPB, typename ST, int CLM = 0>
+// FO selects the function objects: 0 none; 1 those whose pointers in p.fo
+// are set (checked per field at run time); 2 exactly S, SMean, k and kMean
+// (the checks resolved at compile time, which measured 3% faster).
+template <int Q, int TX, int TY, int NSTAGE, int FO, typename MeanT, bool MON, int NPB, typename ST, int CLM = 0>
 __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepParams<MeanT, ST> &p, int bx, int by,
                                             int bz, unsigned g0, const CtaSmem<ST> &sh, int *s_abort, MonAcc &acc,
                                             int item = -1, int mesh = -1, FusedMlp *mlp = nullptr,
@@ -423,6 +426,7 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
     using PG = PopGroups<Q>;
     using C = PopCell<Q, TX, TY, ST>;
     static_assert(PG::d_plane(PG::NG) == XY<Q>::N, "population-plane groups cover the x-y movers");
+    constexpr bool FO4 = FO == 2;  // S, SMean, k, kMean present, momentsMean absent
     const int my_cell = (ty + 1) * G::PX + tx + 1;
 
     // first planes of the item (the slots were last read by ordinary loads)
@@ -467,14 +471,14 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
         }
         // the network runs for the planes this CTA updates (z0 .. z1-1)
         const bool net_plane = (i >= 1) && (i <= nplanes - 2);
-        if constexpr (FO) {
+        if constexpr (FO != 0) {
             if (upd) {
-                if (p.fo.SMean) {
+                if (FO4 || p.fo.SMean) {
 #pragma unroll
                     for (int c = 0; c < 6; c++)
                         sm_old[c] = (p.fo.SMean + c * N)[iu];
                 }
-                if (p.fo.kMean)
+                if (FO4 || p.fo.kMean)
                     km_old = p.fo.kMean[iu];
             }
         }
@@ -601,7 +605,7 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
 #pragma unroll
                 for (int k = 1; k < 10; k++)
                     (p.out + k * N)[iu] = Storage<ST>::store_raw(m[k]);
-                if constexpr (Storage<ST>::SC != 1.0f && (MON || FO)) {
+                if constexpr (Storage<ST>::SC != 1.0f && (MON || FO != 0)) {
                     // the monitor and the function objects take the moments unscaled
 #pragma unroll
                     for (int k = 1; k < 10; k++)
@@ -613,29 +617,29 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
                     const float chk = (((m[0] + m[1]) + (m[2] + m[3])) + ((m[4] + m[5]) + (m[6] + m[7]))) + (m[8] + m[9]);
                     acc.bad += !isfinite(chk);
                 }
-                if constexpr (FO) {
-                    if (p.fo.S || p.fo.SMean) {
+                if constexpr (FO != 0) {
+                    if (FO4 || p.fo.S || p.fo.SMean) {
                         float s6[6];
                         strain_rate(m, p.fo.sd, s6);
-                        if (p.fo.S) {
+                        if (FO4 || p.fo.S) {
 #pragma unroll
                             for (int c = 0; c < 6; c++)
                                 (p.fo.S + c * N)[iu] = s6[c];
                         }
-                        if (p.fo.SMean) {
+                        if (FO4 || p.fo.SMean) {
 #pragma unroll
                             for (int c = 0; c < 6; c++)
                                 (p.fo.SMean + c * N)[iu] = time_average<MeanT>(sm_old[c], MeanT(s6[c]), p.fo.inv_count);
                         }
                     }
-                    if (p.fo.k || p.fo.kMean) {
+                    if (FO4 || p.fo.k || p.fo.kMean) {
                         const float ke = kinetic(m[1], m[2], m[3]);
-                        if (p.fo.k)
+                        if (FO4 || p.fo.k)
                             p.fo.k[iu] = ke;
-                        if (p.fo.kMean)
+                        if (FO4 || p.fo.kMean)
                             p.fo.kMean[iu] = time_average<MeanT>(km_old, MeanT(ke), p.fo.inv_count);
                     }
-                    if (p.fo.momentsMean) {
+                    if (!FO4 && p.fo.momentsMean) {
                         m[0] = m[0] - 1.0f;
 #pragma unroll
                         for (int c = 0; c < 10; c++) {
@@ -681,7 +685,7 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
         return true;
     };
 
-    if constexpr (FO || CLM == 2) {
+    if constexpr (FO != 0 || CLM == 2) {
         // with the function objects or the fused network the body is large:
         // one plane per trip, the up-mover sets rotated by register moves
         // (two unrolled copies of these bodies measured slower)
@@ -760,7 +764,7 @@ __device__ __forceinline__ void drain_after_abort(uint64_t *bars)
 }
 
 // One step of one mesh: CTA (bx, by, bz) of the grid marches its work item.
-template <int Q, int TX, int TY, int NSTAGE, bool FO, typename MeanT, bool MON = false, int NPB = 2, int MINB = 2,
+template <int Q, int TX, int TY, int NSTAGE, int FO, typename MeanT, bool MON = false, int NPB = 2, int MINB = 2,
           typename ST = float>
 __global__ void __launch_bounds__(TX *TY, MINB)
     step_kernel(const __grid_constant__ CUtensorMap tmap_in, const StepParams<MeanT, ST> p)

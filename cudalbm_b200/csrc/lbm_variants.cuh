@@ -31,20 +31,37 @@ constexpr Variant kVariants[] = {
     {27, 16, 8, 2, 1, 1}, {19, 32, 8, 2, 1, 2}, {19, 32, 8, 3, 1, 2}, {19, 16, 8, 2, 1, 2}, {27, 32, 8, 2, 1, 2},
     {27, 16, 8, 2, 1, 2}};
 
-bool pick_q19_f32(int tx, int ty, int stages, int npb, bool fo, int mean_bits, Launcher &out);
-bool pick_q27_f32(int tx, int ty, int stages, int npb, bool fo, int mean_bits, Launcher &out);
-bool pick_f16(int Q, int tx, int ty, int stages, int npb, bool fo, int mean_bits, Launcher &out);
-bool pick_bf16(int Q, int tx, int ty, int stages, int npb, bool fo, int mean_bits, Launcher &out);
+// fo: the handle's function-object bits (LBM_FO_*).
+bool pick_q19_f32(int tx, int ty, int stages, int npb, unsigned fo, int mean_bits, Launcher &out);
+bool pick_q27_f32(int tx, int ty, int stages, int npb, unsigned fo, int mean_bits, Launcher &out);
+bool pick_f16(int Q, int tx, int ty, int stages, int npb, unsigned fo, int mean_bits, Launcher &out);
+bool pick_bf16(int Q, int tx, int ty, int stages, int npb, unsigned fo, int mean_bits, Launcher &out);
 
 #ifdef __CUDACC__
-template <int Q, int TX, int TY, int NS, bool FO, typename MeanT, bool MON, int NPB, int MINB, typename ST>
+template <int Q, int TX, int TY, int NS, int FO, typename MeanT, bool MON, int NPB, int MINB, typename ST>
 void *kernel_fn()
 {
     return reinterpret_cast<void *>(&step_kernel<Q, TX, TY, NS, FO, MeanT, MON, NPB, MINB, ST>);
 }
 
+// The function-object kernel for a set of function objects: none; exactly
+// S, SMean, k and kMean (code 2: no run-time checks); any other set (code 1).
+constexpr unsigned kFoFour = 0x0Fu;  // LBM_FO_S | LBM_FO_SMEAN | LBM_FO_K | LBM_FO_KMEAN
+
+template <int Q, int TX, int TY, int NS, int NPB, int MINB, typename ST, int FO>
+void pick_means(Launcher &l, int mean_bits)
+{
+    if (mean_bits == 64) {
+        l.fn = kernel_fn<Q, TX, TY, NS, FO, double, false, NPB, MINB, ST>();
+        l.fn_mon = kernel_fn<Q, TX, TY, NS, FO, double, true, NPB, MINB, ST>();
+    } else {
+        l.fn = kernel_fn<Q, TX, TY, NS, FO, float, false, NPB, MINB, ST>();
+        l.fn_mon = kernel_fn<Q, TX, TY, NS, FO, float, true, NPB, MINB, ST>();
+    }
+}
+
 template <int Q, int TX, int TY, int NS, int NPB, int MINB, typename ST>
-Launcher pick_fo(bool fo, int mean_bits)
+Launcher pick_fo(unsigned fo, int mean_bits)
 {
     Launcher l;
     l.tx = TX;
@@ -53,14 +70,12 @@ Launcher pick_fo(bool fo, int mean_bits)
     l.pop_buffers = NPB;
     l.smem = SmemLayout<Q, TX, TY, NS, NPB, ST>::bytes;
     if (!fo) {
-        l.fn = kernel_fn<Q, TX, TY, NS, false, float, false, NPB, MINB, ST>();
-        l.fn_mon = kernel_fn<Q, TX, TY, NS, false, float, true, NPB, MINB, ST>();
-    } else if (mean_bits == 64) {
-        l.fn = kernel_fn<Q, TX, TY, NS, true, double, false, NPB, MINB, ST>();
-        l.fn_mon = kernel_fn<Q, TX, TY, NS, true, double, true, NPB, MINB, ST>();
+        l.fn = kernel_fn<Q, TX, TY, NS, 0, float, false, NPB, MINB, ST>();
+        l.fn_mon = kernel_fn<Q, TX, TY, NS, 0, float, true, NPB, MINB, ST>();
+    } else if (fo == kFoFour) {
+        pick_means<Q, TX, TY, NS, NPB, MINB, ST, 2>(l, mean_bits);
     } else {
-        l.fn = kernel_fn<Q, TX, TY, NS, true, float, false, NPB, MINB, ST>();
-        l.fn_mon = kernel_fn<Q, TX, TY, NS, true, float, true, NPB, MINB, ST>();
+        pick_means<Q, TX, TY, NS, NPB, MINB, ST, 1>(l, mean_bits);
     }
     return l;
 }

@@ -4,7 +4,7 @@
 
 namespace lbm {
 
-bool pick_q19_f32(int tx, int ty, int stages, int npb, bool fo, int mean_bits, Launcher &out)
+bool pick_q19_f32(int tx, int ty, int stages, int npb, unsigned fo, int mean_bits, Launcher &out)
 {
     constexpr int Q = 19;
     LBM_VARIANT(19, 32, 8, 2, 1, 1, 3, float)

@@ -4,7 +4,7 @@
 
 namespace lbm {
 
-bool pick_q27_f32(int tx, int ty, int stages, int npb, bool fo, int mean_bits, Launcher &out)
+bool pick_q27_f32(int tx, int ty, int stages, int npb, unsigned fo, int mean_bits, Launcher &out)
 {
     constexpr int Q = 27;
     LBM_VARIANT(27, 32, 8, 2, 1, 1, 3, float)
