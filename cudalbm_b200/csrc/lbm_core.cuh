@@ -601,16 +601,21 @@ struct StrainDiv {
 
 // S_ab = 3 (u_a u_b - m_ab) / (2 scale tau) for the six components
 // (xx, xy, xz, yy, yz, zz) of the stored moments m (u = m[1..3]).
+// The roundings are written out (intrinsics) as the reference's compiled
+// kernel performs them -- 3 * fma(u_a, u_b, -m_ab) -- so that no contraction
+// or sharing of u_a u_b with other formulas in this kernel can change them
+// (tests/test_reference_rounding.py checks the form on the reference's
+// golden outputs).
 __device__ __forceinline__ void strain_rate(const float *m, const StrainDiv &sd, float *S)
 {
     const float u = m[1], v = m[2], w = m[3];
     float x[6];
-    x[0] = 3.0f * ((u * u) - m[4]);
-    x[1] = 3.0f * ((u * v) - m[5]);
-    x[2] = 3.0f * ((u * w) - m[6]);
-    x[3] = 3.0f * ((v * v) - m[7]);
-    x[4] = 3.0f * ((v * w) - m[8]);
-    x[5] = 3.0f * ((w * w) - m[9]);
+    x[0] = __fmul_rn(3.0f, __fmaf_rn(u, u, -m[4]));
+    x[1] = __fmul_rn(3.0f, __fmaf_rn(u, v, -m[5]));
+    x[2] = __fmul_rn(3.0f, __fmaf_rn(u, w, -m[6]));
+    x[3] = __fmul_rn(3.0f, __fmaf_rn(v, v, -m[7]));
+    x[4] = __fmul_rn(3.0f, __fmaf_rn(v, w, -m[8]));
+    x[5] = __fmul_rn(3.0f, __fmaf_rn(w, w, -m[9]));
     const unsigned worst = max(max(max(div_unsafe(x[0]), div_unsafe(x[1])), max(div_unsafe(x[2]), div_unsafe(x[3]))),
                                max(div_unsafe(x[4]), div_unsafe(x[5])));
     if (worst < 128u) {
@@ -631,10 +636,13 @@ __device__ __forceinline__ void strain_rate(const float *m, const StrainDiv &sd,
 }
 __device__ __forceinline__ float kinetic(float u, float v, float w)
 {
-    // a node at rest (+0, the sum of squares is never -0) skips the square
+    // sqrtf((u*u) + (v*v) + (w*w)) * 0.5 as the reference's kernel rounds it:
+    // v*v alone, then u*u and w*w each fused into the sum (intrinsics, so the
+    // form does not depend on this kernel's other uses of the products).  A
+    // node at rest (+0, the sum of squares is never -0) skips the square
     // root: sqrtf(+0) * 0.5 = +0, and a zero argument takes sqrtf's slow path
-    const float s = (u * u) + (v * v) + (w * w);
-    return s == 0.0f ? 0.0f : sqrtf(s) * 0.5f;
+    const float s = __fmaf_rn(w, w, __fmaf_rn(u, u, __fmul_rn(v, v)));
+    return s == 0.0f ? 0.0f : __fmul_rn(sqrtf(s), 0.5f);
 }
 template <typename T>
 __device__ __forceinline__ T time_average(T mean, T f, T inv)
