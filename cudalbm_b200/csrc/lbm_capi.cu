@@ -750,6 +750,8 @@ lbm_status lbm_init_regions(lbm_handle *h, const float region[70])
     lbm_status s = ensure_scratch(h, 70 * sizeof(float));
     if (s != LBM_OK)
         return s;
+    h->last_input_kept = false;  // the state is replaced (see lbm_closure_dtau)
+    h->dtau_current = h->dtau_current && !h->closure;
     LBM_CUDA(cudaMemcpyAsync(h->scratch, region, 70 * sizeof(float), cudaMemcpyHostToDevice, h->stream));
     const int nx = int(h->cfg.nx), ny = int(h->cfg.ny), nz = int(h->cfg.nz);
     const float *rg = static_cast<float *>(h->scratch);
@@ -789,6 +791,10 @@ lbm_status lbm_write_fields(lbm_handle *h, lbm_field_set set, const void *host, 
     lbm_status s = field_ptr(h, set, &dptr, &is_double);
     if (s != LBM_OK)
         return s;
+    if (set == LBM_FIELDS_MOMENTS) {
+        h->last_input_kept = false;  // the state is replaced (see lbm_closure_dtau)
+        h->dtau_current = h->dtau_current && !h->closure;
+    }
     const Xfer x = xfer_of(h, set, dtype, is_double, order);
     if (x.direct) {
         // same values, order and type on both sides: one copy
@@ -1333,6 +1339,8 @@ lbm_status lbm_autotune(lbm_handle *h, int32_t trial_steps, lbm_tuning *out)
         h->cur = cur0;
         h->t = t0;
         h->closure_steps = closure_steps0;
+        h->last_input_kept = false;  // trial steps overwrote the other buffer
+        h->dtau_current = false;     // and, on the separate path, dtau[]
         live[0].first = h->m[cur0];
         for (size_t i = 0; i < live.size(); i++)
             cudaMemcpyAsync(live[i].first, backup[i], live[i].second, cudaMemcpyDeviceToDevice, h->stream);

@@ -544,6 +544,7 @@ lbm_status closure_step(lbm_handle *h)
         LBM_CUDA_RETURN(cudaLaunchKernel(ffn, grid, block, args, fsmem, h->stream));
         h->closure_steps++;
         h->dtau_current = false;
+        h->last_input_kept = true;
         h->cur = nxt;
         h->t += 1;
         h->launches += 1;
@@ -1055,10 +1056,13 @@ lbm_status lbm_closure_dtau(lbm_handle *h, float *host, size_t count)
     LBM_CUDA_RETURN(cudaSetDevice(h->cfg.device));
     if (!h->dtau_current) {
         // the last step evaluated the network inside the step kernel: the
-        // same network on that step's input state (the other moment buffer)
-        // gives its dtau, bit for bit
-        lbm_status s = launch_infer(static_cast<const float *>(h->m[h->cur ^ 1]), h->N, *h->mlp, h->dtau,
-                                    &h->err->flags, true, false, h->stream, h->cfg.device);
+        // same network on that step's input state (the other moment buffer,
+        // while nothing has overwritten it) gives its dtau bit for bit;
+        // otherwise the state has been replaced since, and the network on
+        // the current state gives the dtau the next step will use
+        const void *src = h->last_input_kept ? h->m[h->cur ^ 1] : h->m[h->cur];
+        lbm_status s = launch_infer(static_cast<const float *>(src), h->N, *h->mlp, h->dtau, &h->err->flags, true,
+                                    false, h->stream, h->cfg.device);
         if (s != LBM_OK)
             return s;
         h->launches += 1;

@@ -58,6 +58,7 @@ struct lbm_handle {
     uint64_t closure_steps = 0;        // closure steps taken since lbm_closure_set
     bool closure_fused = true;         // evaluate the network inside the step kernel (when every == 1)
     bool dtau_current = true;          // dtau[] holds the last closure step's values
+    bool last_input_kept = false;      // m[cur ^ 1] is still the input of the last (fused) closure step
 };
 
 namespace lbm {

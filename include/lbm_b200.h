@@ -379,7 +379,10 @@ lbm_status lbm_closure_set(lbm_handle *h, const lbm_mlp *net);
  * between -- a lagged closure for runs where it varies slowly. */
 lbm_status lbm_closure_refresh(lbm_handle *h, int32_t every);
 
-/* The dtau field of the last closure step ([z][y][x], count = nodes). */
+/* The dtau field of the last closure step ([z][y][x], count = nodes).  After
+ * the state has been replaced since that step (lbm_write_fields of the
+ * moments, lbm_init_regions, lbm_autotune), or before any closure step, it
+ * is the field the next step will use. */
 lbm_status lbm_closure_dtau(lbm_handle *h, float *host, size_t count);
 
 /* Where the network runs when it is evaluated every step: on (the default)

@@ -217,6 +217,13 @@ def test_fused_network_equals_separate_kernels(samples, q, nx):
         assert np.count_nonzero(db) > 0  # the network changes tau somewhere
         assert np.array_equal(bits(da), bits(db))
         assert np.array_equal(bits(a.read()), bits(b.read()))
+        # a replaced state: both report the field the next step will use
+        state = a.read()
+        state[1] *= np.float32(0.5)
+        for c in (a, b):
+            c.write(state)
+        da2, db2 = a.closure_dtau(), b.closure_dtau()
+        assert np.array_equal(bits(da2), bits(db2)) and not np.array_equal(bits(da2), bits(da))
 
 
 def test_autotune_picks_the_closure_evaluation_and_keeps_the_state(samples):
