@@ -34,7 +34,8 @@ EXPORTS = ("lbm_config_default", "lbm_create", "lbm_destroy", "lbm_init_regions"
            "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_cavity", "lbm_batch_step", "lbm_batch_synchronize",
            "lbm_batch_autotune", "lbm_batch_get_info", "lbm_batch_configure", "lbm_cut_plane",
            "lbm_vts_write", "lbm_perturb_velocity", "lbm_filter_2to1", "lbm_trainer_create", "lbm_trainer_destroy",
-           "lbm_trainer_add", "lbm_trainer_samples", "lbm_trainer_fit", "lbm_trainer_gradient", "lbm_mlp_infer",
+           "lbm_trainer_add", "lbm_trainer_add_window", "lbm_trainer_samples", "lbm_trainer_fit",
+           "lbm_trainer_gradient", "lbm_mlp_infer",
            "lbm_closure_set", "lbm_closure_dtau", "lbm_closure_refresh", "lbm_closure_fused",
            "lbm_selftest_wait_timeout", "lbm_field_statistics")
 
@@ -163,6 +164,8 @@ def lib() -> ctypes.CDLL:
         L.lbm_trainer_create.argtypes = [i32, u64, ctypes.POINTER(vp)]
         L.lbm_trainer_destroy.argtypes = [vp]
         L.lbm_trainer_add.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.c_float, ctypes.POINTER(u64)]
+        L.lbm_trainer_add_window.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float,
+                                             ctypes.POINTER(u64)]
         L.lbm_trainer_samples.argtypes = [vp, u64, u64, vp, vp, ctypes.POINTER(u64)]
         L.lbm_trainer_fit.argtypes = [vp, ctypes.POINTER(TrainOptions), ctypes.POINTER(MLP), ctypes.POINTER(TrainReport)]
         L.lbm_trainer_gradient.argtypes = [vp, ctypes.POINTER(MLP), u64, u64, ctypes.POINTER(MLP),
@@ -183,7 +186,7 @@ def lib() -> ctypes.CDLL:
                      "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_cavity", "lbm_batch_step",
                      "lbm_batch_synchronize", "lbm_batch_autotune", "lbm_batch_get_info", "lbm_batch_configure",
                      "lbm_cut_plane", "lbm_vts_write", "lbm_perturb_velocity", "lbm_filter_2to1",
-                     "lbm_trainer_create", "lbm_trainer_destroy", "lbm_trainer_add", "lbm_trainer_samples",
+                     "lbm_trainer_create", "lbm_trainer_destroy", "lbm_trainer_add", "lbm_trainer_add_window", "lbm_trainer_samples",
                      "lbm_trainer_fit", "lbm_trainer_gradient", "lbm_mlp_infer", "lbm_closure_set",
                      "lbm_closure_dtau", "lbm_closure_refresh", "lbm_closure_fused", "lbm_selftest_wait_timeout",
                      "lbm_field_statistics"):

@@ -51,6 +51,14 @@ class Trainer:
                                               ctypes.byref(total)))
         return total.value
 
+    def add_window(self, coarse, fine, window: int, stride: int = 1, min_neq: float = 0.0) -> int:
+        """Samples fitted to `window` coarse steps: `coarse` holds the filtered
+        state of `fine`, which this advances by 2 x window steps."""
+        total = ctypes.c_uint64()
+        _lib.check(_lib.lib().lbm_trainer_add_window(self._t, coarse._h, fine._h, int(window), int(stride),
+                                                     float(min_neq), ctypes.byref(total)))
+        return total.value
+
     def __len__(self) -> int:
         total = ctypes.c_uint64()
         _lib.check(_lib.lib().lbm_trainer_samples(self._t, 0, 0, None, None, ctypes.byref(total)))

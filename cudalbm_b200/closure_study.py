@@ -11,7 +11,9 @@ Steps (all on the GPU through the library):
     ``snapshots`` times each is box-filtered 2:1 onto the coarse grid (the
     non-equilibrium stress rescaled to the coarse lattice), the coarse solver
     takes one step from it, and every ``stride``-th interior node gives a
-    sample (16 features, target dtau; lbm_trainer_add).
+    sample (16 features, target dtau; lbm_trainer_add).  With ``window`` > 1
+    each sample's dtau is fitted to that many consecutive coarse steps, each
+    from the filtered fine state (lbm_trainer_add_window).
  2. Training: 16 -> 32 -> 32 -> 1 GELU network, Adam, on the GPU.
  3. Calibration: the network's output is shrunk by the factor in
     ``shrink`` that minimises the centreline error of a coarse run against
@@ -96,7 +98,7 @@ def run_study(nc: int = 128, lattice: int = 27, u_lid: float = 0.05, tau_coarse:
               coarse_steps: int = 10000, seeds: int = 8, snapshots: int = 6, stride: int = 3,
               min_neq: float = 3e-4, train_steps: int = 3000, batch: int = 16384, lr: float = 2e-3,
               dtau_range: Sequence[float] = (0.0, 0.05), shrink: Sequence[float] = (1.0, 0.5, 0.25),
-              device: int = 0, save: str = "", field_pos_max: int = 512,
+              device: int = 0, save: str = "", field_pos_max: int = 512, window: int = 1,
               log: Callable[[str], None] = print) -> Dict[str, object]:
     """``field_pos_max``: largest fine edge for which the whole fine field is
     read back to sample it at the coarse nodes (field_pos); above it only
@@ -129,9 +131,12 @@ def run_study(nc: int = 128, lattice: int = 27, u_lid: float = 0.05, tau_coarse:
                                    sample_at_coarse_nodes(f.read()[1:4], nc) if whole_field else None)
                 if trainer is not None and s in snaps:
                     c.filter_from(f)
-                    f.step(2)
-                    done += 2
-                    trainer.add(c, f, stride=stride, min_neq=min_neq)
+                    if window == 1:
+                        f.step(2)
+                        trainer.add(c, f, stride=stride, min_neq=min_neq)
+                    else:  # one dtau per node fitted to `window` coarse steps
+                        trainer.add_window(c, f, window, stride=stride, min_neq=min_neq)
+                    done += 2 * window
             f.step(Tf - done)
             f.synchronize()
             out["wall"] = time.perf_counter() - t0
@@ -204,7 +209,7 @@ def run_study(nc: int = 128, lattice: int = 27, u_lid: float = 0.05, tau_coarse:
     out = {
         "config": {"lattice": f"D3Q{lattice}", "coarse": nc, "fine": nf, "Re": Re, "tau_coarse": tau_coarse,
                    "u_lid": u_lid, "coarse_steps": Tc, "fine_steps": Tf, "seeds": seeds, "snapshots": snapshots,
-                   "stride": stride, "min_neq": min_neq, "dtau_range": list(dtau_range)},
+                   "stride": stride, "min_neq": min_neq, "dtau_range": list(dtau_range), "window": window},
         "training": {"samples": int(len(targ)), "generation_s": gen_s, "train_s": train_s, "steps": train_steps,
                      "loss_first": rep["loss_first"], "loss_last": rep["loss_last"], "r2_held_out": r2,
                      "shrink_scores": {str(k): v for k, v in scores.items()}, "shrink": best},
@@ -230,13 +235,14 @@ def main():
     ap.add_argument("--dtau-range", default="0,0.05", help="clip of the targets and of the output, lo,hi")
     ap.add_argument("--shrink", default="1,0.5,0.25", help="output scale factors tried in the calibration "
                     "(0 = the plain method)")
+    ap.add_argument("--window", type=int, default=1, help="coarse steps each sample's dtau is fitted to (1: one step)")
     ap.add_argument("--save", default="", help="write the trained network (.npz)")
     ap.add_argument("--json", default="", help="write the results")
     a = ap.parse_args()
     res = run_study(nc=a.nc, coarse_steps=a.coarse_steps, seeds=a.seeds, train_steps=a.train_steps,
                     snapshots=a.snapshots, stride=a.stride, save=a.save,
                     dtau_range=[float(v) for v in a.dtau_range.split(",")],
-                    shrink=[float(v) for v in a.shrink.split(",")])
+                    shrink=[float(v) for v in a.shrink.split(",")], window=a.window)
     text = json.dumps(res, indent=1, default=float)
     if a.json:
         with open(a.json, "w") as fh:

@@ -123,11 +123,30 @@ float refinement_kappa(const lbm_handle *fine, const lbm_handle *coarse)
 // stress for a stable ratio, or an unusable relaxation rate).
 struct TargetArgs {
     const float *f0, *f1, *c;
+    const double *acc;  // per node (sum r.neq, sum neq.neq) over a window of transitions, or null
     int nx, ny, nz;
     unsigned stride;
     float omega, tau0, r_ii, r_ij;
     double min_den;
 };
+// One transition's least-squares terms at node i: r . neq and neq . neq over
+// the six second-order moments (r = F(t+1) - C, neq = C's non-equilibrium part).
+__device__ void transition_terms(const TargetArgs &a, size_t i, size_t N, double &num, double &den)
+{
+    float cm[10];
+    for (int k = 0; k < 10; k++)
+        cm[k] = a.c[size_t(k) * N + i];
+    const float u = cm[1], v = cm[2], w = cm[3];
+    const float eq[6] = {0.5f * u * u, u * v, u * w, 0.5f * v * v, v * w, 0.5f * w * w};
+    num = 0.0;
+    den = 0.0;
+    for (int k = 0; k < 6; k++) {
+        const double neq = double(cm[4 + k]) - double(eq[k]);
+        const double r = double(a.f1[size_t(4 + k) * N + i] - cm[4 + k]);
+        num += r * neq;
+        den += neq * neq;
+    }
+}
 __device__ bool node_target(const TargetArgs &a, size_t i, float &dtau)
 {
     const size_t N = size_t(a.nx) * a.ny * a.nz;
@@ -136,17 +155,12 @@ __device__ bool node_target(const TargetArgs &a, size_t i, float &dtau)
     const int x = int(i % a.nx), y = int((i / a.nx) % a.ny), z = int(i / (size_t(a.nx) * a.ny));
     if (lbm::node_type(x, y, z, a.nx, a.ny, a.nz))
         return false;
-    float cm[10];
-    for (int k = 0; k < 10; k++)
-        cm[k] = a.c[size_t(k) * N + i];
-    const float u = cm[1], v = cm[2], w = cm[3];
-    const float eq[6] = {0.5f * u * u, u * v, u * w, 0.5f * v * v, v * w, 0.5f * w * w};
-    double num = 0.0, den = 0.0;
-    for (int k = 0; k < 6; k++) {
-        const double neq = double(cm[4 + k]) - double(eq[k]);
-        const double r = double(a.f1[size_t(4 + k) * N + i] - cm[4 + k]);
-        num += r * neq;
-        den += neq * neq;
+    double num, den;
+    if (a.acc) {
+        num = a.acc[2 * i];
+        den = a.acc[2 * i + 1];
+    } else {
+        transition_terms(a, i, N, num, den);
     }
     if (!(den > a.min_den))
         return false;
@@ -155,6 +169,21 @@ __device__ bool node_target(const TargetArgs &a, size_t i, float &dtau)
         return false;
     dtau = float(1.0 / w_new - double(a.tau0));
     return isfinite(dtau);
+}
+
+// Adds one transition's terms to the window sums of every interior node.
+__global__ void accumulate_terms_kernel(TargetArgs a, double *acc)
+{
+    const size_t N = size_t(a.nx) * a.ny * a.nz;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x) {
+        const int x = int(i % a.nx), y = int((i / a.nx) % a.ny), z = int(i / (size_t(a.nx) * a.ny));
+        if (lbm::node_type(x, y, z, a.nx, a.ny, a.nz))
+            continue;
+        double num, den;
+        transition_terms(a, i, N, num, den);
+        acc[2 * i] += num;
+        acc[2 * i + 1] += den;
+    }
 }
 
 // Samples are stored in node order, whatever the scheduling: CTA b owns the
@@ -659,6 +688,74 @@ lbm_status lbm_trainer_destroy(lbm_trainer *t)
     return LBM_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+TargetArgs target_args(const lbm_handle *coarse, const float *f0, const float *f1, uint32_t stride, float min_neq,
+                       uint32_t window)
+{
+    TargetArgs a;
+    a.f0 = f0;
+    a.f1 = f1;
+    a.c = static_cast<const float *>(coarse->m[coarse->cur]);
+    a.acc = nullptr;
+    a.nx = int(coarse->cfg.nx);
+    a.ny = int(coarse->cfg.ny);
+    a.nz = int(coarse->cfg.nz);
+    a.stride = stride;
+    a.omega = coarse->omega;
+    a.tau0 = coarse->tau;
+    a.r_ii = 1.0f / (2.0f * 4.5f * coarse->tau);
+    a.r_ij = 1.0f / (2.0f * 9.0f * coarse->tau);
+    // the threshold is on the RMS non-equilibrium stress of a transition
+    a.min_den = std::max(1e-24, 6.0 * double(min_neq) * double(min_neq)) * double(window);
+    return a;
+}
+
+// Count, then write, the samples of targets a (node order) after the stored ones.
+lbm_status store_samples(lbm_trainer *t, lbm_handle *coarse, const TargetArgs &a, uint64_t *total)
+{
+    const size_t N = coarse->N;
+    const size_t ctas = (N + kChunk - 1) / kChunk;
+    if (t->count_slots < ctas) {
+        cudaFree(t->counts);
+        cudaFree(t->offsets);
+        t->counts = nullptr;
+        t->offsets = nullptr;
+        t->count_slots = 0;
+        LBM_CUDA_RETURN(cudaMalloc(&t->counts, ctas * sizeof(unsigned)));
+        LBM_CUDA_RETURN(cudaMalloc(&t->offsets, ctas * sizeof(unsigned long long)));
+        t->count_slots = ctas;
+    }
+    count_samples_kernel<<<unsigned(ctas), kSampleCta, 0, coarse->stream>>>(a, t->counts);
+    LBM_CUDA_RETURN(cudaGetLastError());
+    std::vector<unsigned> counts(ctas);
+    std::vector<unsigned long long> offsets(ctas);
+    LBM_CUDA_RETURN(cudaMemcpyAsync(counts.data(), t->counts, ctas * sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                    coarse->stream));
+    LBM_CUDA_RETURN(cudaStreamSynchronize(coarse->stream));
+    unsigned long long run = t->n;
+    for (size_t b = 0; b < ctas; b++) {
+        offsets[b] = run;
+        run += counts[b];
+    }
+    LBM_CUDA_RETURN(cudaMemcpyAsync(t->offsets, offsets.data(), ctas * sizeof(unsigned long long),
+                                    cudaMemcpyHostToDevice, coarse->stream));
+    write_samples_kernel<<<unsigned(ctas), kSampleCta, 0, coarse->stream>>>(a, t->offsets, t->feat, t->targ, t->cap);
+    LBM_CUDA_RETURN(cudaGetLastError());
+    LBM_CUDA_RETURN(cudaStreamSynchronize(coarse->stream));
+    coarse->launches += 3;
+    t->n = std::min<uint64_t>(run, t->cap);
+    if (total)
+        *total = t->n;
+    return LBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 lbm_status lbm_trainer_add(lbm_trainer *t, lbm_handle *coarse, lbm_handle *fine_next, uint32_t stride, float min_neq,
                            uint64_t *total)
 {
@@ -693,52 +790,65 @@ lbm_status lbm_trainer_add(lbm_trainer *t, lbm_handle *coarse, lbm_handle *fine_
     lbm_status s = lbm_step(coarse, 1);
     if (s != LBM_OK)
         return s;
-    TargetArgs a;
-    a.f0 = f0;
-    a.f1 = f1;
-    a.c = static_cast<const float *>(coarse->m[coarse->cur]);
-    a.nx = int(coarse->cfg.nx);
-    a.ny = int(coarse->cfg.ny);
-    a.nz = int(coarse->cfg.nz);
-    a.stride = stride;
-    a.omega = coarse->omega;
-    a.tau0 = coarse->tau;
-    a.r_ii = 1.0f / (2.0f * 4.5f * coarse->tau);
-    a.r_ij = 1.0f / (2.0f * 9.0f * coarse->tau);
-    a.min_den = std::max(1e-24, 6.0 * double(min_neq) * double(min_neq));
-    const size_t ctas = (N + kChunk - 1) / kChunk;
-    if (t->count_slots < ctas) {
-        cudaFree(t->counts);
-        cudaFree(t->offsets);
-        t->counts = nullptr;
-        t->offsets = nullptr;
-        t->count_slots = 0;
-        LBM_CUDA_RETURN(cudaMalloc(&t->counts, ctas * sizeof(unsigned)));
-        LBM_CUDA_RETURN(cudaMalloc(&t->offsets, ctas * sizeof(unsigned long long)));
-        t->count_slots = ctas;
+    TargetArgs a = target_args(coarse, f0, f1, stride, min_neq, 1);
+    return store_samples(t, coarse, a, total);
+}
+
+lbm_status lbm_trainer_add_window(lbm_trainer *t, lbm_handle *coarse, lbm_handle *fine, uint32_t window,
+                                  uint32_t stride, float min_neq, uint64_t *total)
+{
+    if (!t || !coarse || !fine || stride == 0 || window == 0)
+        return fail(LBM_ERR_ARG, "lbm_trainer_add_window: null argument, zero stride or zero window");
+    if (coarse->closure || coarse->cfg.function_objects || coarse->storage != LBM_STORAGE_F32)
+        return fail(LBM_ERR_ARG, "lbm_trainer_add_window: the coarse handle must run the plain FP32 method without function objects");
+    if (fine->closure || fine->cfg.nx != 2 * coarse->cfg.nx || fine->cfg.ny != 2 * coarse->cfg.ny ||
+        fine->cfg.nz != 2 * coarse->cfg.nz || fine->storage != LBM_STORAGE_F32)
+        return fail(LBM_ERR_ARG, "lbm_trainer_add_window: the fine mesh must be twice the coarse mesh (plain FP32)");
+    if (coarse->cfg.device != t->device || fine->cfg.device != t->device)
+        return fail(LBM_ERR_ARG, "lbm_trainer_add_window: handles on another device");
+    LBM_CUDA_RETURN(cudaSetDevice(t->device));
+    const size_t N = coarse->N;
+    // F(t) (the features), F(t+j+1), and the per-node window sums (2 doubles)
+    const size_t need = 24 * N;
+    if (t->scratch_floats < need) {
+        if (t->scratch)
+            cudaFree(t->scratch);
+        t->scratch = nullptr;
+        t->scratch_floats = 0;
+        LBM_CUDA_RETURN(cudaMalloc(&t->scratch, need * sizeof(float)));
+        t->scratch_floats = need;
     }
-    count_samples_kernel<<<unsigned(ctas), kSampleCta, 0, coarse->stream>>>(a, t->counts);
-    LBM_CUDA_RETURN(cudaGetLastError());
-    std::vector<unsigned> counts(ctas);
-    std::vector<unsigned long long> offsets(ctas);
-    LBM_CUDA_RETURN(cudaMemcpyAsync(counts.data(), t->counts, ctas * sizeof(unsigned), cudaMemcpyDeviceToHost,
+    float *fstart = t->scratch, *f1 = t->scratch + 10 * N;
+    double *acc = reinterpret_cast<double *>(t->scratch + 20 * N);
+    LBM_CUDA_RETURN(cudaStreamSynchronize(fine->stream));
+    LBM_CUDA_RETURN(cudaStreamSynchronize(coarse->stream));
+    LBM_CUDA_RETURN(cudaMemcpyAsync(fstart, coarse->m[coarse->cur], 10 * N * sizeof(float), cudaMemcpyDeviceToDevice,
                                     coarse->stream));
-    LBM_CUDA_RETURN(cudaStreamSynchronize(coarse->stream));
-    unsigned long long run = t->n;
-    for (size_t b = 0; b < ctas; b++) {
-        offsets[b] = run;
-        run += counts[b];
+    LBM_CUDA_RETURN(cudaMemsetAsync(acc, 0, 2 * N * sizeof(double), coarse->stream));
+    const int nx = int(coarse->cfg.nx), ny = int(coarse->cfg.ny), nz = int(coarse->cfg.nz);
+    const float kappa = refinement_kappa(fine, coarse);
+    for (uint32_t j = 0; j < window; j++) {
+        // the coarse handle holds F(t+j); the fine run advances one coarse step
+        lbm_status s = lbm_step(fine, 2);
+        if (s != LBM_OK)
+            return s;
+        LBM_CUDA_RETURN(cudaStreamSynchronize(fine->stream));
+        filter_kernel<<<grid_for(N), 256, 0, coarse->stream>>>(f1, static_cast<const float *>(fine->m[fine->cur]), nx,
+                                                               ny, nz, kappa);
+        LBM_CUDA_RETURN(cudaGetLastError());
+        if ((s = lbm_step(coarse, 1)) != LBM_OK)  // C: one coarse step from F(t+j)
+            return s;
+        TargetArgs a = target_args(coarse, fstart, f1, stride, min_neq, window);
+        accumulate_terms_kernel<<<grid_for(N), 256, 0, coarse->stream>>>(a, acc);
+        LBM_CUDA_RETURN(cudaGetLastError());
+        coarse->launches += 2;
+        if (j + 1 < window)  // the next transition starts from the filtered F(t+j+1)
+            LBM_CUDA_RETURN(cudaMemcpyAsync(coarse->m[coarse->cur], f1, 10 * N * sizeof(float),
+                                            cudaMemcpyDeviceToDevice, coarse->stream));
     }
-    LBM_CUDA_RETURN(cudaMemcpyAsync(t->offsets, offsets.data(), ctas * sizeof(unsigned long long),
-                                    cudaMemcpyHostToDevice, coarse->stream));
-    write_samples_kernel<<<unsigned(ctas), kSampleCta, 0, coarse->stream>>>(a, t->offsets, t->feat, t->targ, t->cap);
-    LBM_CUDA_RETURN(cudaGetLastError());
-    LBM_CUDA_RETURN(cudaStreamSynchronize(coarse->stream));
-    coarse->launches += 3;
-    t->n = std::min<uint64_t>(run, t->cap);
-    if (total)
-        *total = t->n;
-    return LBM_OK;
+    TargetArgs a = target_args(coarse, fstart, f1, stride, min_neq, window);
+    a.acc = acc;
+    return store_samples(t, coarse, a, total);
 }
 
 lbm_status lbm_trainer_samples(lbm_trainer *t, uint64_t first, uint64_t count, float *features, float *targets,

@@ -349,6 +349,19 @@ lbm_status lbm_trainer_destroy(lbm_trainer *t);
 lbm_status lbm_trainer_add(lbm_trainer *t, lbm_handle *coarse, lbm_handle *fine_next, uint32_t stride,
                            float min_neq, uint64_t *total);
 
+/* Samples whose target fits one dtau per node to a window of `window`
+ * consecutive coarse steps: the coarse handle holds the filtered state F(t)
+ * of the fine run (whose current time is 2t); the call advances the fine run
+ * by 2 x window steps and, for each j, one plain coarse step from F(t+j),
+ * comparing it with F(t+j+1); per node it sums the least-squares terms of
+ * every transition (residual . non-equilibrium stress, non-equilibrium
+ * stress squared) and stores one sample: the features of F(t) and the dtau
+ * of the summed terms.  window = 1 gives the samples of lbm_trainer_add.
+ * The coarse handle is left at the last transition's coarse step.
+ * Replaces: nothing in the reference (no closure). */
+lbm_status lbm_trainer_add_window(lbm_trainer *t, lbm_handle *coarse, lbm_handle *fine, uint32_t window,
+                                  uint32_t stride, float min_neq, uint64_t *total);
+
 /* Copy stored samples [first, first+count) to the host (features [n][16],
  * targets [n]; either may be NULL); *total = samples stored. */
 lbm_status lbm_trainer_samples(lbm_trainer *t, uint64_t first, uint64_t count, float *features, float *targets,

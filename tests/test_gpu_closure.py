@@ -244,3 +244,40 @@ def test_autotune_picks_the_closure_evaluation_and_keeps_the_state(samples):
             c.synchronize()
         assert b.info()["step"] == 8
         assert np.array_equal(bits(a.read()), bits(b.read()))
+
+
+def window_samples(window, q=27, n=32, steps=40):
+    """Samples of one snapshot of a perturbed fine run: lbm_trainer_add
+    (window 0 here) or lbm_trainer_add_window."""
+    tr = Trainer(capacity=200000)
+    with Cavity(q, n, n, n, 400.0, 0.05) as fine, Cavity(q, n // 2, n // 2, n // 2, 400.0, 0.05) as coarse:
+        fine.init_regions()
+        fine.perturb_velocity(1e-3, 0)
+        fine.step(steps)
+        coarse.filter_from(fine)
+        if window == 0:
+            fine.step(2)
+            tr.add(coarse, fine)
+        else:
+            tr.add_window(coarse, fine, window)
+        fine.synchronize()
+        assert fine.info()["step"] == steps + 2 * max(window, 1)
+        out = tr.samples()
+    tr.close()
+    return out
+
+
+def test_window_targets():
+    """A window of one coarse step gives exactly lbm_trainer_add's samples; a
+    window of four fits one dtau per node to four transitions (same features
+    at the window's start, finite targets that differ)."""
+    f0, t0 = window_samples(0)
+    f1, t1 = window_samples(1)
+    assert len(t0) > 1000
+    assert np.array_equal(f0.view(np.uint32), f1.view(np.uint32))
+    assert np.array_equal(t0.view(np.uint32), t1.view(np.uint32))
+    f4, t4 = window_samples(4)
+    assert len(t4) > 1000 and np.all(np.isfinite(t4))
+    common = min(len(t0), len(t4))
+    assert not np.array_equal(t4[:common], t0[:common])
+    assert np.std(t4) < np.std(t0)  # the window averages out transition noise
