@@ -29,7 +29,7 @@ constexpr Variant kVariants[] = {
     {19, 16, 8, 2, 1, 0}, {19, 8, 8, 2, 1, 0},  {27, 32, 8, 2, 1, 0}, {27, 32, 8, 2, 2, 0}, {27, 16, 8, 2, 1, 0},
     {27, 8, 8, 2, 1, 0},  {19, 32, 8, 2, 1, 1}, {19, 32, 8, 3, 1, 1}, {19, 16, 8, 2, 1, 1}, {27, 32, 8, 2, 1, 1},
     {27, 16, 8, 2, 1, 1}, {19, 32, 8, 2, 1, 2}, {19, 32, 8, 3, 1, 2}, {19, 16, 8, 2, 1, 2}, {27, 32, 8, 2, 1, 2},
-    {27, 16, 8, 2, 1, 2}};
+    {27, 16, 8, 2, 1, 2}, {19, 32, 8, 2, 4, 1}, {19, 32, 8, 2, 4, 2}};
 
 // fo: the handle's function-object bits (LBM_FO_*).
 bool pick_q19_f32(int tx, int ty, int stages, int npb, unsigned fo, int mean_bits, Launcher &out);

@@ -7,6 +7,7 @@ namespace lbm {
 bool pick_f16(int Q, int tx, int ty, int stages, int npb, unsigned fo, int mean_bits, Launcher &out)
 {
     LBM_VARIANT(19, 32, 8, 2, 1, 1, 3, __half)
+    LBM_VARIANT(19, 32, 8, 2, 4, 1, 4, __half)
     LBM_VARIANT(19, 32, 8, 3, 1, 1, 3, __half)
     LBM_VARIANT(19, 16, 8, 2, 1, 1, 3, __half)
     LBM_VARIANT(27, 32, 8, 2, 1, 1, 3, __half)
