@@ -7,19 +7,23 @@
 //      multi-stage shared-memory ring, completion tracked by an mbarrier;
 //   2. reconstructs the populations of its nodes (and, on the ring, only the
 //      ones that point into the tile) and writes the ones that move in x-y
-//      into a double-buffered shared-memory plane;
-//   3. after one CTA barrier, pulls f_q(x) = R_q(m(x - c_q)) for every
+//      into a shared-memory population plane (one or two buffers), grouped
+//      by in-plane step (cx, cy): per group one float cell for the
+//      down-mover and one float2 cell for the same-plane and up-movers;
+//   3. after a CTA barrier, pulls f_q(x) = R_q(m(x - c_q)) for every
 //      direction: x-y movers from shared memory, pure-z movers and the rest
 //      population from registers of the previous/next plane;
 //   4. updates the plane below (whose three source planes are now complete):
 //      boundary or interior moments, scale, collide, store, and the fused
-//      function objects S, k and their running means.
+//      function objects S, k and their running means (and, in the closure
+//      kernels, the relaxation time from the learned network).
 // No population ever goes to global memory: the reference's block-halo faces
 // (src/blockHalo/halo.cuh) are replaced by the moment ring, which neighbour
 // CTAs read at the same time from L2.
 //
 // Moments live in two global buffers (read A, write B, swap each step) laid
-// out as [field][z][y][x] float32 -- x fastest, 10 fields of nx*ny*nz.
+// out as [field][z][y][x] -- x fastest, 10 fields of nx*ny*nz, in the storage
+// format (FP32, or FP16/BF16: see Storage).
 #pragma once
 
 #include <cuda.h>
