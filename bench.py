@@ -223,7 +223,23 @@ def link_ceiling(device: int):
                 ms = e0.elapsed_time(e1)
                 best = ms if best is None else min(best, ms)
             out[key] = round(n / (best / 1e3) / 1e9, 2)
-        del h, d
+        # both directions at once (what an overlapped job sees): 1 GiB each way
+        h2 = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+        d2 = torch.empty(n, dtype=torch.uint8, device=dev)
+        s1, s2 = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+        best = None
+        for _ in range(3):
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            with torch.cuda.stream(s1):
+                d.copy_(h, non_blocking=True)
+            with torch.cuda.stream(s2):
+                h2.copy_(d2, non_blocking=True)
+            torch.cuda.synchronize(dev)
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+        out["duplex_each_way"] = round(n / best / 1e9, 2)
+        del h, d, h2, d2
         torch.cuda.empty_cache()
         return out
     except Exception as exc:  # reported, never silent
@@ -289,6 +305,7 @@ def run_ours(args, w):
                                  else np.float32) for fs in ("moments",) + tuple(w["fo"])}
     mon = _lib.PinnedArray((args.steps,), np.dtype(_lib.MONITOR_DTYPE))
     link = link_ceiling(local)
+    # (a) the calls one after the other: upload, K monitored steps, download
     barrier()
     cav.synchronize()
     t0 = time.perf_counter()
@@ -302,12 +319,30 @@ def run_ours(args, w):
         cav.read(fs, out=buf.array)
     t3 = time.perf_counter()
     barrier()
-    e2e_s = max_over_ranks(t3 - t0)
-    e2e = world * nodes * args.steps / e2e_s / 1e6
+    seq_s = max_over_ranks(t3 - t0)
     h2d = 10 * nodes * 4
     d2h = sum(b.array.nbytes for b in outs.values())
     copy_gbs = {"h2d": round(h2d / (t1 - t0) / 1e9, 2), "d2h": round(d2h / (t3 - t2) / 1e9, 2)}
     red = {"mass": float(mon.array[-1]["mass"]), "nonfinite": int(mon.array["nonfinite"].max())}
+    # (b) the same job as one lbm_run_streamed call: the upload, the steps
+    # and the download overlap (z-slabs of each step shifted by the step
+    # index); FP32 storage only.  One untimed call first (streams, events).
+    streamed = w.get("storage", "f32") == "f32"
+    e2e_s = seq_s
+    if streamed:
+        host_outs = {fs: b.array for fs, b in outs.items()}
+        cav.run_streamed(state.array, min(args.steps, 4), host_outs, monitor=mon.array, slab=args.stream_slab,
+                         z_chunk=args.stream_zc)
+        barrier()
+        cav.synchronize()
+        t4 = time.perf_counter()
+        cav.run_streamed(state.array, args.steps, host_outs, monitor=mon.array, slab=args.stream_slab,
+                         z_chunk=args.stream_zc)
+        t5 = time.perf_counter()
+        barrier()
+        e2e_s = max_over_ranks(t5 - t4)
+        red = {"mass": float(mon.array[-1]["mass"]), "nonfinite": int(mon.array["nonfinite"].max())}
+    e2e = world * nodes * args.steps / e2e_s / 1e6
     cav.close()
     group.close()
 
@@ -340,13 +375,24 @@ def run_ours(args, w):
                      "bytes_per_node_alg": w["b_alg"], "peak_kind": f"of {peak_kind}"},
         "e2e": {"value": round(e2e, 2), "unit": "MLUPS", "h2d_bytes_per_step": round(h2d / args.steps),
                 "d2h_bytes_per_step": round(24 + d2h / args.steps),
-                "what": "lbm_write_fields (pinned h2d of the state) + K x lbm_step_monitored (each step's 24 B "
-                        "FP64 mass/energy/non-finite sums copied back) + lbm_read_fields of moments and "
-                        "function objects",
-                "seconds": {"h2d": round(t1 - t0, 5), "steps": round(t2 - t1, 5), "d2h": round(t3 - t2, 5)},
-                "copy_gbs": copy_gbs, "link_gbs": link,
+                "what": ("one lbm_run_streamed call: pinned h2d of the state, K steps (each step's 24 B FP64 "
+                         "mass/energy/non-finite sums), d2h of the moments and function objects, the copies "
+                         "overlapping the steps" if streamed else
+                         "lbm_write_fields (pinned h2d of the state) + K x lbm_step_monitored (each step's 24 B "
+                         "FP64 mass/energy/non-finite sums copied back) + lbm_read_fields of moments and "
+                         "function objects"),
+                "seconds": round(e2e_s, 5),
+                "sequential": {"value": round(world * nodes * args.steps / seq_s / 1e6, 2),
+                               "what": "the same transfers and steps as separate calls, one after the other",
+                               "seconds": {"h2d": round(t1 - t0, 5), "steps": round(t2 - t1, 5),
+                                           "d2h": round(t3 - t2, 5)},
+                               "copy_gbs": copy_gbs},
+                "link_gbs": link,
                 "copy_frac_of_link": ({k: round(copy_gbs[k] / link[k], 3) for k in ("h2d", "d2h")}
-                                      if link else None)},
+                                      if link else None),
+                "transfer_bound_mlups": (round(nodes * args.steps / (max(h2d / (link["h2d"] * 1e9),
+                                                                         d2h / (link["d2h"] * 1e9))) / 1e6, 1)
+                                         if link else None)},
         "gpu_launches": int(launches),
         "clocks": clocks,
         "check": {"mass_last_step": red["mass"], "nonfinite_max": red["nonfinite"]},
@@ -678,6 +724,8 @@ def main():
     ap.add_argument("--pop-buffers", type=int, default=0)
     ap.add_argument("--no-autotune", action="store_true", help="keep the default kernel variant")
     ap.add_argument("--tune-steps", type=int, default=10)
+    ap.add_argument("--stream-slab", type=int, default=0, help="lbm_run_streamed slab height (0: default)")
+    ap.add_argument("--stream-zc", type=int, default=0, help="lbm_run_streamed z-chunk (0: default)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -30,8 +30,8 @@ F32, F64 = 0, 1
 EXPORTS = ("lbm_config_default", "lbm_create", "lbm_destroy", "lbm_init_regions", "lbm_write_fields",
            "lbm_read_fields", "lbm_step", "lbm_synchronize", "lbm_reduce", "lbm_get_info", "lbm_last_error",
            "lbm_status_string", "lbm_field_set_vars", "lbm_host_alloc", "lbm_host_free", "lbm_case_read",
-           "lbm_lbmbin_write", "lbm_reduce_moments_noalloc", "lbm_step_monitored", "lbm_autotune",
-           "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_cavity", "lbm_batch_step", "lbm_batch_synchronize",
+           "lbm_lbmbin_write", "lbm_reduce_moments_noalloc", "lbm_step_monitored", "lbm_run_streamed",
+           "lbm_autotune", "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_cavity", "lbm_batch_step", "lbm_batch_synchronize",
            "lbm_batch_autotune", "lbm_batch_get_info", "lbm_batch_configure", "lbm_cut_plane",
            "lbm_vts_write", "lbm_perturb_velocity", "lbm_filter_2to1", "lbm_trainer_create", "lbm_trainer_destroy",
            "lbm_trainer_add", "lbm_trainer_add_window", "lbm_trainer_samples", "lbm_trainer_fit",
@@ -63,6 +63,10 @@ class Tuning(ctypes.Structure):
     _fields_ = [("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32), ("z_chunk", ctypes.c_int32),
                 ("stages", ctypes.c_int32), ("pop_buffers", ctypes.c_int32), ("ms_per_step", ctypes.c_double),
                 ("candidates", ctypes.c_int32), ("from_cache", ctypes.c_int32), ("closure_fused", ctypes.c_int32)]
+
+
+class StreamOpts(ctypes.Structure):
+    _fields_ = [("slab", ctypes.c_int32), ("z_chunk", ctypes.c_int32)]
 
 
 class BatchInfo(ctypes.Structure):
@@ -147,6 +151,7 @@ def lib() -> ctypes.CDLL:
         L.lbm_case_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(Case)]
         L.lbm_reduce_moments_noalloc.argtypes = [vp, u64, ctypes.POINTER(ctypes.c_double), vp]
         L.lbm_step_monitored.argtypes = [vp, u64, vp]
+        L.lbm_run_streamed.argtypes = [vp, vp, u64, ctypes.POINTER(vp), vp, ctypes.POINTER(StreamOpts)]
         L.lbm_autotune.argtypes = [vp, i32, ctypes.POINTER(Tuning)]
         L.lbm_batch_create.argtypes = [ctypes.POINTER(Config), i32, ctypes.POINTER(vp)]
         L.lbm_batch_destroy.argtypes = [vp]
@@ -182,8 +187,8 @@ def lib() -> ctypes.CDLL:
                                        i32]
         for name in ("lbm_create", "lbm_destroy", "lbm_init_regions", "lbm_write_fields", "lbm_read_fields",
                      "lbm_step", "lbm_synchronize", "lbm_reduce", "lbm_get_info", "lbm_host_alloc", "lbm_host_free",
-                     "lbm_case_read", "lbm_lbmbin_write", "lbm_reduce_moments_noalloc", "lbm_step_monitored", "lbm_autotune",
-                     "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_cavity", "lbm_batch_step",
+                     "lbm_case_read", "lbm_lbmbin_write", "lbm_reduce_moments_noalloc", "lbm_step_monitored",
+                     "lbm_run_streamed", "lbm_autotune", "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_cavity", "lbm_batch_step",
                      "lbm_batch_synchronize", "lbm_batch_autotune", "lbm_batch_get_info", "lbm_batch_configure",
                      "lbm_cut_plane", "lbm_vts_write", "lbm_perturb_velocity", "lbm_filter_2to1",
                      "lbm_trainer_create", "lbm_trainer_destroy", "lbm_trainer_add", "lbm_trainer_add_window", "lbm_trainer_samples",

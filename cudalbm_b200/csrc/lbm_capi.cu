@@ -495,6 +495,8 @@ lbm_status launch_step(lbm_handle *h, bool monitored = false)
     p.ny = int(h->cfg.ny);
     p.nz = int(h->cfg.nz);
     p.zc = h->zc;
+    p.z_lo = 0;
+    p.z_hi = p.nz;
     p.rx = lbm::Relax{h->omega, h->t_omega, h->omega_d2, h->tau, h->cfg.u_inf};
     p.fo.S = h->S;
     p.fo.SMean = static_cast<MeanT *>(h->SMean);
@@ -523,6 +525,47 @@ lbm_status launch_step(lbm_handle *h, bool monitored = false)
                               h->stream));
     h->cur = nxt;
     h->t += 1;
+    h->launches += 1;
+    return LBM_OK;
+}
+
+// Step t of the planes [z_lo, z_hi) only, reading buffer `in` and writing the
+// other one (lbm_run_streamed); mon: the step's monitor slot or null.  The
+// handle's step counter and buffer index are left alone.
+template <typename MeanT>
+lbm_status launch_slab(lbm_handle *h, int in, int64_t t, int z_lo, int z_hi, int zc, lbm::MonitorSlot *mon)
+{
+    StepParams<MeanT> p{};
+    p.out = static_cast<float *>(h->m[in ^ 1]);
+    p.mon = mon;
+    p.nx = int(h->cfg.nx);
+    p.ny = int(h->cfg.ny);
+    p.nz = int(h->cfg.nz);
+    p.zc = zc;
+    p.z_lo = z_lo;
+    p.z_hi = z_hi;
+    p.rx = lbm::Relax{h->omega, h->t_omega, h->omega_d2, h->tau, h->cfg.u_inf};
+    p.fo.S = h->S;
+    p.fo.SMean = static_cast<MeanT *>(h->SMean);
+    p.fo.k = h->k;
+    p.fo.kMean = static_cast<MeanT *>(h->kMean);
+    p.fo.momentsMean = static_cast<MeanT *>(h->momentsMean);
+    if constexpr (std::is_same_v<MeanT, float>)
+        p.fo.inv_count = 1.0f / static_cast<float>(t + 1);
+    else
+        p.fo.inv_count = 1.0 / static_cast<double>(t + 1);
+    p.fo.sd.d_ii = 2.0f * 4.5f * h->tau;
+    p.fo.sd.d_ij = 2.0f * 9.0f * h->tau;
+    p.fo.sd.r_ii = 1.0f / p.fo.sd.d_ii;
+    p.fo.sd.r_ij = 1.0f / p.fo.sd.d_ij;
+    p.fault = h->err;
+    p.timeout_ns = 2000000000ull;
+    const dim3 block(h->launcher.tx, h->launcher.ty);
+    const dim3 grid(unsigned((h->cfg.nx + h->launcher.tx - 1) / h->launcher.tx),
+                    unsigned((h->cfg.ny + h->launcher.ty - 1) / h->launcher.ty), unsigned((z_hi - z_lo + zc - 1) / zc));
+    void *args[] = {&h->tmap[in], &p};
+    LBM_CUDA(cudaLaunchKernel(mon ? h->launcher.fn_mon : h->launcher.fn, grid, block, args, h->launcher.smem,
+                              h->stream));
     h->launches += 1;
     return LBM_OK;
 }
@@ -564,9 +607,14 @@ void destroy_handle(lbm_handle *h)
         cudaStreamSynchronize(h->stream);
     for (void *p : {h->m[0], h->m[1], static_cast<void *>(h->S), static_cast<void *>(h->k), h->SMean, h->kMean,
                     h->momentsMean, static_cast<void *>(h->err), static_cast<void *>(h->red),
-                    static_cast<void *>(h->mon), h->scratch, static_cast<void *>(h->dtau)})
+                    static_cast<void *>(h->mon), h->scratch, static_cast<void *>(h->dtau),
+                    static_cast<void *>(h->mon_steps)})
         if (p)
             cudaFree(p);
+    if (h->dstream) {
+        cudaStreamSynchronize(h->dstream);
+        cudaStreamDestroy(h->dstream);
+    }
     delete h->mlp;
     if (h->steps_graph)
         cudaGraphExecDestroy(h->steps_graph);
@@ -988,6 +1036,159 @@ lbm_status lbm_step_monitored(lbm_handle *h, uint64_t n, lbm_monitor *out)
     LBM_CUDA(cudaEventRecord(h->ev1, h->stream));
     h->timed = true;
     return LBM_OK;
+}
+
+lbm_status lbm_run_streamed(lbm_handle *h, const float *moments, uint64_t n, void *const out[6], lbm_monitor *mon,
+                            const lbm_stream_opts *opts)
+{
+    if (!h || !moments || !out)
+        return fail(LBM_ERR_ARG, "null argument");
+    if (n == 0 || n > uint64_t(1) << 30)
+        return fail(LBM_ERR_ARG, "lbm_run_streamed: n must be in [1, 2^30]");
+    if (h->storage != 0 || h->closure)
+        return fail(LBM_ERR_STATE, "lbm_run_streamed: FP32 storage without the learned closure only");
+    const int P = opts && opts->slab > 0 ? opts->slab : 16;
+    const int zc = opts && opts->z_chunk > 0 ? std::min(opts->z_chunk, P) : std::min(4, P);
+    if (P > (1 << 20))
+        return fail(LBM_ERR_ARG, "lbm_run_streamed: slab too large");
+    // host buffers and the device field of every requested set
+    struct Out {
+        char *host;
+        char *dev;
+        size_t esz;
+        int nv;
+    };
+    std::vector<Out> outs;
+    for (int s = 0; s < 6; s++) {
+        if (!out[s] || s == LBM_FIELDS_MOMENTS)
+            continue;
+        void *d = nullptr;
+        int is_double = 0;
+        lbm_status st = field_ptr(h, lbm_field_set(s), &d, &is_double);
+        if (st != LBM_OK)
+            return st;
+        outs.push_back({static_cast<char *>(out[s]), static_cast<char *>(d), size_t(is_double ? 8 : 4),
+                        nvars_of(lbm_field_set(s))});
+    }
+    LBM_CUDA(cudaSetDevice(h->cfg.device));
+    if (!h->xstream)
+        LBM_CUDA(cudaStreamCreateWithFlags(&h->xstream, cudaStreamNonBlocking));
+    if (!h->dstream)
+        LBM_CUDA(cudaStreamCreateWithFlags(&h->dstream, cudaStreamNonBlocking));
+    if (mon && h->mon_steps_cap < n) {
+        if (h->mon_steps) {
+            cudaFree(h->mon_steps);
+            h->device_bytes -= h->mon_steps_cap * sizeof(lbm::MonitorSlot);
+            h->mon_steps = nullptr;
+            h->mon_steps_cap = 0;
+        }
+        LBM_CUDA(cudaMalloc(&h->mon_steps, n * sizeof(lbm::MonitorSlot)));
+        h->mon_steps_cap = n;
+        h->device_bytes += n * sizeof(lbm::MonitorSlot);
+    }
+    const int nz = int(h->cfg.nz);
+    const size_t plane = size_t(h->cfg.nx) * size_t(h->cfg.ny);
+    const size_t pitch = h->N * sizeof(float);
+    const int U = (nz + P - 1) / P;                                  // upload chunks of P planes
+    const int J = int((uint64_t(nz) + n - 1 + uint64_t(P) - 1) / uint64_t(P));  // slabs
+    const int in0 = h->cur;
+    const int fin = int((uint64_t(in0) + n) & 1u);  // buffer of the final moments
+    std::vector<cudaEvent_t> evs(size_t(U) + size_t(J) + 1, nullptr);
+    auto cleanup = [&] {
+        for (cudaEvent_t e : evs)
+            if (e)
+                cudaEventDestroy(e);
+    };
+    for (auto &e : evs) {
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            cleanup();
+            return fail(LBM_ERR_CUDA, "lbm_run_streamed: event creation failed");
+        }
+    }
+    cudaEvent_t *up = evs.data(), *done = evs.data() + U, start = evs[size_t(U) + size_t(J)];
+    lbm_status st = LBM_OK;
+    auto run = [&]() -> lbm_status {
+        // the copies must not overtake work already queued on the handle
+        LBM_CUDA(cudaEventRecord(start, h->stream));
+        LBM_CUDA(cudaStreamWaitEvent(h->xstream, start, 0));
+        LBM_CUDA(cudaStreamWaitEvent(h->dstream, start, 0));
+        // uploads: chunk u = planes [u P, (u+1) P) of all 10 fields
+        char *dst0 = static_cast<char *>(h->m[in0]);
+        for (int u = 0; u < U; u++) {
+            const size_t z0 = size_t(u) * P, z1 = std::min<size_t>(nz, z0 + P);
+            const size_t off = z0 * plane * sizeof(float);
+            LBM_CUDA(cudaMemcpy2DAsync(dst0 + off, pitch, reinterpret_cast<const char *>(moments) + off, pitch,
+                                       (z1 - z0) * plane * sizeof(float), 10, cudaMemcpyHostToDevice, h->xstream));
+            LBM_CUDA(cudaEventRecord(up[u], h->xstream));
+        }
+        if (mon)
+            LBM_CUDA(cudaMemsetAsync(h->mon_steps, 0, n * sizeof(lbm::MonitorSlot), h->stream));
+        LBM_CUDA(cudaEventRecord(h->ev0, h->stream));
+        const bool md = means_f64(h);
+        int waited = -1;
+        for (int j = 0; j < J; j++) {
+            // step 0 of slab j reads planes up to (j+1) P
+            const int need = std::min(U - 1, j + 1);
+            for (; waited < need; waited++)
+                LBM_CUDA(cudaStreamWaitEvent(h->stream, up[waited + 1], 0));
+            for (uint64_t s = 0; s < n; s++) {
+                const int64_t lo = std::max<int64_t>(0, int64_t(j) * P - int64_t(s));
+                const int64_t hi = std::min<int64_t>(nz, int64_t(j + 1) * P - int64_t(s));
+                if (lo >= hi)
+                    continue;
+                const int in = int((uint64_t(in0) + s) & 1u);
+                lbm::MonitorSlot *slot = mon ? h->mon_steps + s : nullptr;
+                lbm_status ls = md ? launch_slab<double>(h, in, h->t + int64_t(s), int(lo), int(hi), zc, slot)
+                                   : launch_slab<float>(h, in, h->t + int64_t(s), int(lo), int(hi), zc, slot);
+                if (ls != LBM_OK)
+                    return ls;
+            }
+            LBM_CUDA(cudaEventRecord(done[j], h->stream));
+            // planes whose last step slab j completed
+            const int64_t flo = std::max<int64_t>(0, int64_t(j) * P - int64_t(n) + 1);
+            const int64_t fhi = std::min<int64_t>(nz, int64_t(j + 1) * P - int64_t(n) + 1);
+            if (flo >= fhi)
+                continue;
+            LBM_CUDA(cudaStreamWaitEvent(h->dstream, done[j], 0));
+            const size_t z0 = size_t(flo), nzs = size_t(fhi - flo);
+            if (out[LBM_FIELDS_MOMENTS]) {
+                const size_t off = z0 * plane * sizeof(float);
+                LBM_CUDA(cudaMemcpy2DAsync(static_cast<char *>(out[LBM_FIELDS_MOMENTS]) + off, pitch,
+                                           static_cast<const char *>(h->m[fin]) + off, pitch,
+                                           nzs * plane * sizeof(float), 10, cudaMemcpyDeviceToHost, h->dstream));
+            }
+            for (const Out &o : outs) {
+                const size_t off = z0 * plane * o.esz;
+                LBM_CUDA(cudaMemcpy2DAsync(o.host + off, h->N * o.esz, o.dev + off, h->N * o.esz,
+                                           nzs * plane * o.esz, size_t(o.nv), cudaMemcpyDeviceToHost, h->dstream));
+            }
+        }
+        LBM_CUDA(cudaEventRecord(h->ev1, h->stream));
+        if (mon) {
+            LBM_CUDA(cudaStreamWaitEvent(h->dstream, done[J - 1], 0));
+            LBM_CUDA(cudaMemcpyAsync(mon, h->mon_steps, n * sizeof(lbm::MonitorSlot), cudaMemcpyDeviceToHost,
+                                     h->dstream));
+        }
+        return LBM_OK;
+    };
+    st = run();
+    // wait for everything queued, also after an error in the middle
+    const cudaError_t e1 = cudaStreamSynchronize(h->dstream);
+    const cudaError_t e2 = cudaStreamSynchronize(h->xstream);
+    const cudaError_t e3 = cudaStreamSynchronize(h->stream);
+    cleanup();
+    if (st != LBM_OK)
+        return st;
+    for (cudaError_t e : {e1, e2, e3})
+        if (e != cudaSuccess)
+            return fail(LBM_ERR_CUDA, std::string("lbm_run_streamed: ") + cudaGetErrorString(e));
+    h->cur = fin;
+    h->t += int64_t(n);
+    h->timed = true;
+    h->last_input_kept = false;
+    lbm::StepFault f{};
+    LBM_CUDA(cudaMemcpy(&f, h->err, sizeof(f), cudaMemcpyDeviceToHost));
+    return lbm::check_fault(f, "a step kernel");
 }
 
 lbm_status lbm_synchronize(lbm_handle *h)

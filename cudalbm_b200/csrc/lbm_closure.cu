@@ -561,6 +561,8 @@ lbm_status closure_step(lbm_handle *h)
         p.ny = int(h->cfg.ny);
         p.nz = int(h->cfg.nz);
         p.zc = h->zc;
+        p.z_lo = 0;
+        p.z_hi = p.nz;
         p.rx = Relax{h->omega, h->t_omega, h->omega_d2, h->tau, h->cfg.u_inf};
         p.fault = h->err;
         p.timeout_ns = 2000000000ull;
@@ -598,6 +600,8 @@ lbm_status closure_step(lbm_handle *h)
     p.ny = int(h->cfg.ny);
     p.nz = int(h->cfg.nz);
     p.zc = h->zc;
+    p.z_lo = 0;
+    p.z_hi = p.nz;
     p.rx = Relax{h->omega, h->t_omega, h->omega_d2, h->tau, h->cfg.u_inf};
     p.fault = h->err;
     p.timeout_ns = 2000000000ull;

@@ -40,6 +40,11 @@ struct lbm_handle {
     cudaStream_t xstream = nullptr;
     cudaEvent_t xe_copied[2] = {nullptr, nullptr};
     cudaEvent_t xe_converted[2] = {nullptr, nullptr};
+    // lbm_run_streamed: uploads go on xstream, downloads on dstream; one
+    // monitor slot per step of the job
+    cudaStream_t dstream = nullptr;
+    lbm::MonitorSlot *mon_steps = nullptr;
+    size_t mon_steps_cap = 0;
     float tau = 0, omega = 0, t_omega = 0, omega_d2 = 0;
     int64_t t = 0;
     lbm::Launcher launcher;

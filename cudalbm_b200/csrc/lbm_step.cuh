@@ -148,6 +148,7 @@ struct StepParams {
     MonitorSlot *mon;  // per-step sums (monitored kernels only)
     int nx, ny, nz;
     int zc;            // z-planes per CTA
+    int z_lo, z_hi;    // planes this launch updates: CTA bz takes [z_lo + bz zc, min(z_lo + (bz+1) zc, z_hi))
     Relax rx;
     FOPtrs<MeanT> fo;
     StepFault *fault;
@@ -416,8 +417,8 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int lin = ty * TX + tx;
     const int x0 = bx * TX, y0 = by * TY;
-    const int z0 = bz * p.zc;
-    const int z1 = min(z0 + p.zc, p.nz);
+    const int z0 = p.z_lo + bz * p.zc;
+    const int z1 = min(z0 + p.zc, p.z_hi);
     const int nplanes = z1 - z0 + 2;  // planes z0-1 .. z1
     const int x = x0 + tx, y = y0 + ty;
     const bool own = (x < p.nx) && (y < p.ny);
@@ -994,6 +995,8 @@ __global__ void __launch_bounds__(TX *TY, MINB) batch_kernel(const BatchParams b
         p.ny = bm.ny;
         p.nz = bm.nz;
         p.zc = bm.zc;
+        p.z_lo = 0;
+        p.z_hi = bm.nz;
         p.rx = bm.rx;
         p.fault = bp.fault;
         p.timeout_ns = bp.timeout_ns;

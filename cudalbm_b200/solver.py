@@ -175,6 +175,31 @@ class Cavity:
         _lib.check(_lib.lib().lbm_step_monitored(self._h, int(n), out.ctypes.data))
         return out
 
+    def run_streamed(self, moments: np.ndarray, n: int, outs: Dict[str, np.ndarray], monitor=None,
+                     slab: int = 0, z_chunk: int = 0) -> None:
+        """One job between host arrays with the copies overlapping the steps:
+        upload ``moments`` ([10, nz, ny, nx] float32), advance ``n`` steps and
+        download each field set named in ``outs`` into its array ([nvars, nz,
+        ny, nx]; float64 for the means of an FP64-mean handle); ``monitor``
+        (structured array of length n, or None) receives the per-step sums.
+        Page-locked arrays (_lib.PinnedArray) let the copies run at full speed."""
+        nz, ny, nx = self.shape
+        if moments.dtype != np.float32 or not moments.flags.c_contiguous or moments.size != 10 * nx * ny * nz:
+            raise ValueError("moments must be a contiguous float32 array of 10 fields")
+        ptrs = (ctypes.c_void_p * 6)()
+        for name, arr in outs.items():
+            want = np.float64 if (self.cfg.mean_bits == 64 and "Mean" in name) else np.float32
+            if arr.dtype != want or not arr.flags.c_contiguous or arr.size != NVARS[name] * nx * ny * nz:
+                raise ValueError(f"output '{name}' must be a contiguous {np.dtype(want).name} array of "
+                                 f"{NVARS[name]} fields")
+            ptrs[_lib.FIELD_SET[name]] = arr.ctypes.data
+        if monitor is not None and (monitor.dtype != np.dtype(_lib.MONITOR_DTYPE) or monitor.size < n):
+            raise ValueError("monitor must be a MONITOR_DTYPE array of at least n entries")
+        opts = _lib.StreamOpts(int(slab), int(z_chunk))
+        _lib.check(_lib.lib().lbm_run_streamed(self._h, moments.ctypes.data, int(n), ptrs,
+                                               monitor.ctypes.data if monitor is not None else None,
+                                               ctypes.byref(opts)))
+
     def autotune(self, trial_steps: int = 10) -> Dict[str, object]:
         """Pick the fastest kernel variant for this size class (state unchanged)."""
         t = _lib.Tuning()

@@ -153,6 +153,40 @@ typedef struct lbm_monitor {
  * (applications/fieldCalculate/fieldCalculate.cuh:74-110), at no extra pass. */
 lbm_status lbm_step_monitored(lbm_handle *h, uint64_t n, lbm_monitor *out);
 
+/* Kernel shape of lbm_run_streamed; 0 in a field picks its default. */
+typedef struct lbm_stream_opts {
+    int32_t slab;      /* planes per slab (default 16) */
+    int32_t z_chunk;   /* planes per CTA inside a slab launch (default 4) */
+} lbm_stream_opts;
+
+/* One whole job between host buffers, with the transfers overlapped with
+ * the steps: upload the 10 moment fields from `moments` (FP32, stored units,
+ * [field][z][y][x]), advance n >= 1 steps, and download the results into
+ * out[set] for set = LBM_FIELDS_MOMENTS ... LBM_FIELDS_MOMENTSMEAN (host
+ * buffers in [field][z][y][x] order, FP32, FP64 for the running means when
+ * mean_bits is 64; NULL skips a set; sets of function objects the handle
+ * does not compute must be NULL).  mon[i] (NULL: none) receives step i's
+ * sums as lbm_step_monitored gives them.  The function-object accumulators
+ * continue from their device values, as after lbm_write_fields of the
+ * moments.  The results are those of lbm_write_fields + lbm_step(n) +
+ * lbm_read_fields, bit for bit (the monitor sums up to FP64 summation
+ * order).
+ * How: the mesh is cut into z-slabs of `slab` planes; slab j of step s is
+ * shifted down by s planes (planes [j slab - s, (j+1) slab - s)), so that it
+ * needs only slabs j-1 and j of step s-1, and all n steps of slab j run
+ * before slab j+1.  The upload of slab j+1 (a second stream) overlaps the
+ * steps of slab j, and the planes that slab j finished (n-1 planes behind
+ * it) are downloaded (a third stream) while slab j+1 runs, so the job takes
+ * about as long as the larger of its two transfers instead of their sum.
+ * Host buffers should be page-locked (lbm_host_alloc); the call returns when
+ * the results are in host memory.  FP32 storage without the learned closure
+ * (LBM_ERR_STATE otherwise).  Replaces: the reference's host-to-device copy
+ * of the initial state, time loop and device-to-host copies at save steps
+ * (momentBasedD3Q19.cu:70-137, src/memory/memory.cuh:157-195), which run
+ * one after the other. */
+lbm_status lbm_run_streamed(lbm_handle *h, const float *moments, uint64_t n, void *const out[6], lbm_monitor *mon,
+                            const lbm_stream_opts *opts);
+
 /* Wait for queued work and report device-side error flags. */
 lbm_status lbm_synchronize(lbm_handle *h);
 
