@@ -11,15 +11,20 @@ time step of the whole cavity.  Prints one JSON line (rank 0).
 * value       MLUPS of the device-timed step loop (CUDA events on the solver's
               stream, inputs resident in HBM; the moment buffers, 1.3 GB, are
               far larger than the 126 MB L2, so no flush is needed).
-* e2e         the same metric through the C ABI with host buffers: upload of
-              the state from pinned host memory, K x lbm_step_monitored (each
-              step's 24-byte FP64 sums -- mass, kinetic energy, non-finite
-              count -- copied back to pinned memory), download of the moments
-              and function objects -- all inside the timed region.
+* e2e         the same metric through the C ABI with host buffers, one
+              lbm_run_streamed call: upload of the state from pinned host
+              memory, K steps (each step's 24-byte FP64 sums -- mass, kinetic
+              energy, non-finite count -- copied back), download of the
+              moments and function objects to pinned memory, the copies
+              overlapping the steps -- all inside the timed region.  The
+              same job as separate calls (lbm_write_fields, K x
+              lbm_step_monitored, lbm_read_fields) is reported beside it.
 * roofline    algorithmic bytes per node update (reference tiling: 134 B for
               D3Q27 + 4 + 24 + 48 + 8 B for k, S, SMean, kMean = 218 B) times
               the nodes per launch over the measured launch time, against the
               measured HBM copy bandwidth.
+* other_workloads  plain D3Q27 / D3Q19 256^3 and D3Q19 64^3, device-timed
+              the same way in the same run (--others '' skips them).
 * cpu_baseline  the FP64 OpenMP CPU oracle (oracle/, a restatement of the
               reference's scheme; the reference has no CPU path) timed on this
               host on the same mesh for a bounded number of steps.
@@ -399,12 +404,55 @@ def run_ours(args, w):
         "kernel": {"tile": [info["tile_x"], info["tile_y"]], "z_chunk": info["z_chunk"], "stages": info["stages"],
                    "autotuned": tuning},
     }
+    if world == 1 and args.others:
+        line["other_workloads"] = other_workloads(args, local)
     if world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(w)
         except Exception as exc:  # reported, never silent
             line["cpu_baseline"] = {"value": None, "error": repr(exc)}
     return line
+
+
+OTHER_WORKLOADS = ("q27_256", "q19_256", "q19_64")
+
+
+def other_workloads(args, local):
+    """The plain-method configurations beside the headline one, device-timed
+    the same way (autotuned, W warm-up steps, K timed steps), so that their
+    numbers come from the same run: D3Q27 and D3Q19 256^3 (the plain FP32
+    roofline targets) and D3Q19 64^3 (the small configuration)."""
+    from cudalbm_b200.solver import Cavity
+
+    peak, peak_kind = hbm_peak()
+    out = []
+    for name in args.others.split(","):
+        w = WORKLOADS[name]
+        nx, ny, nz = w["n"]
+        nodes = nx * ny * nz
+        try:
+            cav = Cavity(w["lattice"], nx, ny, nz, w["Re"], w["u"], function_objects=w["fo"],
+                         mean_bits=w["mean_bits"], device=local, storage=w.get("storage", "f32"))
+            cav.init_regions()
+            cav.autotune(args.tune_steps)
+            cav.step(args.warmup)
+            cav.synchronize()
+            cav.step(args.steps)
+            cav.synchronize()
+            info = cav.info()
+            cav.close()
+        except Exception as exc:  # reported, never silent
+            out.append({"workload": w["desc"], "error": repr(exc)})
+            continue
+        ms_step = info["last_step_ms"] / args.steps
+        achieved = w["b_alg"] * nodes / (ms_step / 1e3) / 1e9
+        out.append({"workload": w["desc"], "value": round(nodes / (ms_step / 1e3) / 1e6, 2), "unit": "MLUPS",
+                    "ms_per_step": round(ms_step, 5), "roofline_frac": round(achieved / peak, 4),
+                    "bytes_per_node_alg": w["b_alg"], "peak_kind": f"of {peak_kind}",
+                    "physical_frac": round(80 * nodes / (ms_step / 1e3) / 1e9 / peak, 4),
+                    "kernel": {"tile": [info["tile_x"], info["tile_y"]], "z_chunk": info["z_chunk"],
+                               "stages": info["stages"]}})
+    return out
 
 
 # ------------------------------------------------------ batched arm
@@ -724,6 +772,8 @@ def main():
     ap.add_argument("--pop-buffers", type=int, default=0)
     ap.add_argument("--no-autotune", action="store_true", help="keep the default kernel variant")
     ap.add_argument("--tune-steps", type=int, default=10)
+    ap.add_argument("--others", default=",".join(OTHER_WORKLOADS),
+                    help="plain workloads also timed (device) in the default run, comma-separated; '' for none")
     ap.add_argument("--stream-slab", type=int, default=0, help="lbm_run_streamed slab height (0: default)")
     ap.add_argument("--stream-zc", type=int, default=0, help="lbm_run_streamed z-chunk (0: default)")
     args = ap.parse_args()

@@ -1089,7 +1089,8 @@ lbm_status lbm_run_streamed(lbm_handle *h, const float *moments, uint64_t n, voi
     const int nz = int(h->cfg.nz);
     const size_t plane = size_t(h->cfg.nx) * size_t(h->cfg.ny);
     const size_t pitch = h->N * sizeof(float);
-    const int U = (nz + P - 1) / P;                                  // upload chunks of P planes
+    const int UP = std::min(P, 4);                                   // planes per upload chunk
+    const int U = (nz + UP - 1) / UP;                                // upload chunks
     const int J = int((uint64_t(nz) + n - 1 + uint64_t(P) - 1) / uint64_t(P));  // slabs
     const int in0 = h->cur;
     const int fin = int((uint64_t(in0) + n) & 1u);  // buffer of the final moments
@@ -1112,10 +1113,11 @@ lbm_status lbm_run_streamed(lbm_handle *h, const float *moments, uint64_t n, voi
         LBM_CUDA(cudaEventRecord(start, h->stream));
         LBM_CUDA(cudaStreamWaitEvent(h->xstream, start, 0));
         LBM_CUDA(cudaStreamWaitEvent(h->dstream, start, 0));
-        // uploads: chunk u = planes [u P, (u+1) P) of all 10 fields
+        // uploads: chunk u = planes [u UP, (u+1) UP) of all 10 fields (small
+        // chunks, so that the first slab starts early)
         char *dst0 = static_cast<char *>(h->m[in0]);
         for (int u = 0; u < U; u++) {
-            const size_t z0 = size_t(u) * P, z1 = std::min<size_t>(nz, z0 + P);
+            const size_t z0 = size_t(u) * UP, z1 = std::min<size_t>(nz, z0 + UP);
             const size_t off = z0 * plane * sizeof(float);
             LBM_CUDA(cudaMemcpy2DAsync(dst0 + off, pitch, reinterpret_cast<const char *>(moments) + off, pitch,
                                        (z1 - z0) * plane * sizeof(float), 10, cudaMemcpyHostToDevice, h->xstream));
@@ -1128,7 +1130,7 @@ lbm_status lbm_run_streamed(lbm_handle *h, const float *moments, uint64_t n, voi
         int waited = -1;
         for (int j = 0; j < J; j++) {
             // step 0 of slab j reads planes up to (j+1) P
-            const int need = std::min(U - 1, j + 1);
+            const int need = int(std::min<int64_t>(nz - 1, int64_t(j + 1) * P) / UP);
             for (; waited < need; waited++)
                 LBM_CUDA(cudaStreamWaitEvent(h->stream, up[waited + 1], 0));
             for (uint64_t s = 0; s < n; s++) {
