@@ -1091,67 +1091,73 @@ lbm_status lbm_run_streamed(lbm_handle *h, const float *moments, uint64_t n, voi
     const size_t pitch = h->N * sizeof(float);
     const int UP = std::min(P, 4);                                   // planes per upload chunk
     const int U = (nz + UP - 1) / UP;                                // upload chunks
-    const int J = int((uint64_t(nz) + n - 1 + uint64_t(P) - 1) / uint64_t(P));  // slabs
     const int in0 = h->cur;
     const int fin = int((uint64_t(in0) + n) & 1u);  // buffer of the final moments
-    std::vector<cudaEvent_t> evs(size_t(U) + size_t(J) + 1, nullptr);
+    // A long job runs its first and last kSkew steps as skewed slabs (the
+    // upload overlaps the first ones, the download the last ones) and the
+    // steps between them as whole-mesh launches; a short one is one skewed
+    // phase with both transfers.
+    constexpr uint64_t kSkew = 16;
+    const bool split = n > 2 * kSkew;
+    std::vector<cudaEvent_t> evs;
     auto cleanup = [&] {
         for (cudaEvent_t e : evs)
-            if (e)
-                cudaEventDestroy(e);
+            cudaEventDestroy(e);
     };
-    for (auto &e : evs) {
-        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
-            cleanup();
+    auto new_event = [&](cudaEvent_t *e) -> lbm_status {
+        if (cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess)
             return fail(LBM_ERR_CUDA, "lbm_run_streamed: event creation failed");
-        }
-    }
-    cudaEvent_t *up = evs.data(), *done = evs.data() + U, start = evs[size_t(U) + size_t(J)];
-    lbm_status st = LBM_OK;
-    auto run = [&]() -> lbm_status {
-        // the copies must not overtake work already queued on the handle
-        LBM_CUDA(cudaEventRecord(start, h->stream));
-        LBM_CUDA(cudaStreamWaitEvent(h->xstream, start, 0));
-        LBM_CUDA(cudaStreamWaitEvent(h->dstream, start, 0));
-        // uploads: chunk u = planes [u UP, (u+1) UP) of all 10 fields (small
-        // chunks, so that the first slab starts early)
-        char *dst0 = static_cast<char *>(h->m[in0]);
-        for (int u = 0; u < U; u++) {
-            const size_t z0 = size_t(u) * UP, z1 = std::min<size_t>(nz, z0 + UP);
-            const size_t off = z0 * plane * sizeof(float);
-            LBM_CUDA(cudaMemcpy2DAsync(dst0 + off, pitch, reinterpret_cast<const char *>(moments) + off, pitch,
-                                       (z1 - z0) * plane * sizeof(float), 10, cudaMemcpyHostToDevice, h->xstream));
-            LBM_CUDA(cudaEventRecord(up[u], h->xstream));
-        }
-        if (mon)
-            LBM_CUDA(cudaMemsetAsync(h->mon_steps, 0, n * sizeof(lbm::MonitorSlot), h->stream));
-        LBM_CUDA(cudaEventRecord(h->ev0, h->stream));
-        const bool md = means_f64(h);
-        int waited = -1;
+        evs.push_back(*e);
+        return LBM_OK;
+    };
+    const bool md = means_f64(h);
+    auto step_range = [&](uint64_t s, int64_t lo, int64_t hi, int zcl) -> lbm_status {
+        const int in = int((uint64_t(in0) + s) & 1u);
+        lbm::MonitorSlot *slot = mon ? h->mon_steps + s : nullptr;
+        return md ? launch_slab<double>(h, in, h->t + int64_t(s), int(lo), int(hi), zcl, slot)
+                  : launch_slab<float>(h, in, h->t + int64_t(s), int(lo), int(hi), zcl, slot);
+    };
+    std::vector<cudaEvent_t> up(size_t(U), nullptr);
+    int waited = -1;  // upload chunks the compute stream has waited for
+    // Steps [s0, s0 + m) as skewed slabs: slab j covers planes [bnd(j),
+    // bnd(j+1)) at its first step and one plane lower at each following
+    // step; the first slab is m + P/2 planes high, so that its own last step
+    // already finishes planes, the others P, up to nz + m - 1.  With
+    // `uploads`, slab j first waits for the chunk that holds plane bnd(j+1);
+    // with `downloads`, the planes slab j finished go to the host after it.
+    auto skewed = [&](uint64_t s0, uint64_t m, bool uploads, bool downloads) -> lbm_status {
+        const int64_t F = int64_t(m) + P / 2;
+        auto bnd = [&](int64_t j) -> int64_t { return j == 0 ? 0 : F + (j - 1) * int64_t(P); };
+        const int64_t span = int64_t(nz) + int64_t(m) - 1;
+        const int J = int(1 + (span > F ? (span - F + P - 1) / P : 0));
         for (int j = 0; j < J; j++) {
-            // step 0 of slab j reads planes up to (j+1) P
-            const int need = int(std::min<int64_t>(nz - 1, int64_t(j + 1) * P) / UP);
-            for (; waited < need; waited++)
-                LBM_CUDA(cudaStreamWaitEvent(h->stream, up[waited + 1], 0));
-            for (uint64_t s = 0; s < n; s++) {
-                const int64_t lo = std::max<int64_t>(0, int64_t(j) * P - int64_t(s));
-                const int64_t hi = std::min<int64_t>(nz, int64_t(j + 1) * P - int64_t(s));
+            if (uploads) {
+                const int need = int(std::min<int64_t>(nz - 1, bnd(j + 1)) / UP);
+                for (; waited < need; waited++)
+                    LBM_CUDA(cudaStreamWaitEvent(h->stream, up[size_t(waited + 1)], 0));
+            }
+            for (uint64_t s = 0; s < m; s++) {
+                const int64_t lo = std::max<int64_t>(0, bnd(j) - int64_t(s));
+                const int64_t hi = std::min<int64_t>(nz, bnd(j + 1) - int64_t(s));
                 if (lo >= hi)
                     continue;
-                const int in = int((uint64_t(in0) + s) & 1u);
-                lbm::MonitorSlot *slot = mon ? h->mon_steps + s : nullptr;
-                lbm_status ls = md ? launch_slab<double>(h, in, h->t + int64_t(s), int(lo), int(hi), zc, slot)
-                                   : launch_slab<float>(h, in, h->t + int64_t(s), int(lo), int(hi), zc, slot);
+                lbm_status ls = step_range(s0 + s, lo, hi, zc);
                 if (ls != LBM_OK)
                     return ls;
             }
-            LBM_CUDA(cudaEventRecord(done[j], h->stream));
+            if (!downloads)
+                continue;
             // planes whose last step slab j completed
-            const int64_t flo = std::max<int64_t>(0, int64_t(j) * P - int64_t(n) + 1);
-            const int64_t fhi = std::min<int64_t>(nz, int64_t(j + 1) * P - int64_t(n) + 1);
+            const int64_t flo = std::max<int64_t>(0, bnd(j) - int64_t(m) + 1);
+            const int64_t fhi = std::min<int64_t>(nz, bnd(j + 1) - int64_t(m) + 1);
             if (flo >= fhi)
                 continue;
-            LBM_CUDA(cudaStreamWaitEvent(h->dstream, done[j], 0));
+            cudaEvent_t done;
+            lbm_status es = new_event(&done);
+            if (es != LBM_OK)
+                return es;
+            LBM_CUDA(cudaEventRecord(done, h->stream));
+            LBM_CUDA(cudaStreamWaitEvent(h->dstream, done, 0));
             const size_t z0 = size_t(flo), nzs = size_t(fhi - flo);
             if (out[LBM_FIELDS_MOMENTS]) {
                 const size_t off = z0 * plane * sizeof(float);
@@ -1165,9 +1171,51 @@ lbm_status lbm_run_streamed(lbm_handle *h, const float *moments, uint64_t n, voi
                                            nzs * plane * o.esz, size_t(o.nv), cudaMemcpyDeviceToHost, h->dstream));
             }
         }
+        return LBM_OK;
+    };
+    lbm_status st = LBM_OK;
+    auto run = [&]() -> lbm_status {
+        cudaEvent_t start, end;
+        lbm_status es = new_event(&start);
+        if (es == LBM_OK)
+            es = new_event(&end);
+        for (size_t u = 0; u < up.size() && es == LBM_OK; u++)
+            es = new_event(&up[u]);
+        if (es != LBM_OK)
+            return es;
+        // the copies must not overtake work already queued on the handle
+        LBM_CUDA(cudaEventRecord(start, h->stream));
+        LBM_CUDA(cudaStreamWaitEvent(h->xstream, start, 0));
+        LBM_CUDA(cudaStreamWaitEvent(h->dstream, start, 0));
+        // uploads: chunk u = planes [u UP, (u+1) UP) of all 10 fields (small
+        // chunks, so that the first slab starts early)
+        char *dst0 = static_cast<char *>(h->m[in0]);
+        for (int u = 0; u < U; u++) {
+            const size_t z0 = size_t(u) * UP, z1 = std::min<size_t>(nz, z0 + UP);
+            const size_t off = z0 * plane * sizeof(float);
+            LBM_CUDA(cudaMemcpy2DAsync(dst0 + off, pitch, reinterpret_cast<const char *>(moments) + off, pitch,
+                                       (z1 - z0) * plane * sizeof(float), 10, cudaMemcpyHostToDevice, h->xstream));
+            LBM_CUDA(cudaEventRecord(up[size_t(u)], h->xstream));
+        }
+        if (mon)
+            LBM_CUDA(cudaMemsetAsync(h->mon_steps, 0, n * sizeof(lbm::MonitorSlot), h->stream));
+        LBM_CUDA(cudaEventRecord(h->ev0, h->stream));
+        lbm_status ps;
+        if (!split) {
+            ps = skewed(0, n, true, true);
+        } else {
+            ps = skewed(0, kSkew, true, false);
+            for (uint64_t s = kSkew; ps == LBM_OK && s < n - kSkew; s++)
+                ps = step_range(s, 0, nz, h->zc);
+            if (ps == LBM_OK)
+                ps = skewed(n - kSkew, kSkew, false, true);
+        }
+        if (ps != LBM_OK)
+            return ps;
         LBM_CUDA(cudaEventRecord(h->ev1, h->stream));
         if (mon) {
-            LBM_CUDA(cudaStreamWaitEvent(h->dstream, done[J - 1], 0));
+            LBM_CUDA(cudaEventRecord(end, h->stream));
+            LBM_CUDA(cudaStreamWaitEvent(h->dstream, end, 0));
             LBM_CUDA(cudaMemcpyAsync(mon, h->mon_steps, n * sizeof(lbm::MonitorSlot), cudaMemcpyDeviceToHost,
                                      h->dstream));
         }

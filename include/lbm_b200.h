@@ -171,13 +171,17 @@ typedef struct lbm_stream_opts {
  * moments.  The results are those of lbm_write_fields + lbm_step(n) +
  * lbm_read_fields, bit for bit (the monitor sums up to FP64 summation
  * order).
- * How: the mesh is cut into z-slabs of `slab` planes; slab j of step s is
- * shifted down by s planes (planes [j slab - s, (j+1) slab - s)), so that it
- * needs only slabs j-1 and j of step s-1, and all n steps of slab j run
- * before slab j+1.  The upload of slab j+1 (a second stream) overlaps the
- * steps of slab j, and the planes that slab j finished (n-1 planes behind
- * it) are downloaded (a third stream) while slab j+1 runs, so the job takes
- * about as long as the larger of its two transfers instead of their sum.
+ * How: the mesh is cut into z-slabs (the first n + slab/2 planes high, so
+ * that its own last step already finishes planes, the others `slab`); slab j
+ * of step s is shifted down by s planes, so that it needs only slabs j-1 and
+ * j of step s-1, and all n steps of slab j run before slab j+1.  The upload
+ * (a second stream, in 4-plane chunks) runs ahead of the slabs, and the
+ * planes that slab j finished (n-1 planes behind its top) are downloaded (a
+ * third stream) while slab j+1 runs, so the job takes about as long as the
+ * larger of its two transfers instead of their sum.  A job of more than 32
+ * steps runs only its first and last 16 steps this way (with the upload and
+ * the download respectively) and the steps between them as whole-mesh
+ * launches.
  * Host buffers should be page-locked (lbm_host_alloc); the call returns when
  * the results are in host memory.  FP32 storage without the learned closure
  * (LBM_ERR_STATE otherwise).  Replaces: the reference's host-to-device copy

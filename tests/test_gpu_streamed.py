@@ -1,5 +1,6 @@
 """lbm_run_streamed: a whole job between host buffers with the copies
-overlapping the steps (z-slabs of each step shifted down by the step index).
+overlapping the steps (z-slabs of each step shifted down by the step index;
+a job longer than 32 steps skews only its first and last 16 steps).
 
 The slab launches update the same nodes with the same arithmetic as whole-mesh
 launches, so moments and function objects must equal those of
@@ -58,6 +59,9 @@ CASES = [
     (19, (32, 32, 40), ("S", "SMean", "k", "kMean", "momentsMean"), 64, 20, 9, 4, 2),
     (27, (32, 32, 64), ("k",), 32, 10, 3, 128, 0),
     (19, (32, 40, 48), (), 32, 5, 1, 0, 0),
+    # long jobs: skewed first and last 16 steps around whole-mesh steps
+    (19, (32, 32, 48), ("S", "SMean", "k", "kMean"), 32, 5, 41, 8, 4),
+    (27, (32, 40, 64), (), 32, 3, 70, 16, 0),
 ]
 
 
