@@ -331,8 +331,8 @@ def run_ours(args, w):
     red = {"mass": float(mon.array[-1]["mass"]), "nonfinite": int(mon.array["nonfinite"].max())}
     # (b) the same job as one lbm_run_streamed call: the upload, the steps
     # and the download overlap (z-slabs of each step shifted by the step
-    # index); FP32 storage only.  One untimed call first (streams, events).
-    streamed = w.get("storage", "f32") == "f32"
+    # index).  One untimed call first (streams, events, staging).
+    streamed = True
     e2e_s = seq_s
     if streamed:
         host_outs = {fs: b.array for fs, b in outs.items()}

@@ -99,6 +99,24 @@ __global__ void moment_out_kernel(H *dst, const ST *src, int k, int nx, int ny, 
     }
 }
 
+// Planes of the 10 moment fields between a contiguous FP32 staging block
+// ([field][cnt nodes]) and the device storage format at node offset `off` of
+// every field (lbm_run_streamed with 16-bit storage); blockIdx.y = field.
+template <typename ST>
+__global__ void planes_in_kernel(ST *m, const float *stage, size_t N, size_t off, size_t cnt)
+{
+    const int k = blockIdx.y;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < cnt; i += size_t(gridDim.x) * blockDim.x)
+        m[size_t(k) * N + off + i] = lbm::Storage<ST>::store(stage[size_t(k) * cnt + i], k);
+}
+template <typename ST>
+__global__ void planes_out_kernel(float *stage, const ST *m, size_t N, size_t off, size_t cnt)
+{
+    const int k = blockIdx.y;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < cnt; i += size_t(gridDim.x) * blockDim.x)
+        stage[size_t(k) * cnt + i] = lbm::Storage<ST>::load(m[size_t(k) * N + off + i], k);
+}
+
 // dst (device layout, global order) <- src (one field of nodes, given order/type)
 template <typename S, typename D>
 __global__ void gather_in_kernel(D *dst, const S *src, int nx, int ny, int nz, int tiled)
@@ -1045,8 +1063,8 @@ lbm_status lbm_run_streamed(lbm_handle *h, const float *moments, uint64_t n, voi
         return fail(LBM_ERR_ARG, "null argument");
     if (n == 0 || n > uint64_t(1) << 30)
         return fail(LBM_ERR_ARG, "lbm_run_streamed: n must be in [1, 2^30]");
-    if (h->storage != 0 || h->closure)
-        return fail(LBM_ERR_STATE, "lbm_run_streamed: FP32 storage without the learned closure only");
+    if (h->closure)
+        return fail(LBM_ERR_STATE, "lbm_run_streamed: not available with the learned closure");
     const int P = opts && opts->slab > 0 ? opts->slab : 16;
     const int zc = opts && opts->z_chunk > 0 ? std::min(opts->z_chunk, P) : std::min(4, P);
     if (P > (1 << 20))
@@ -1091,6 +1109,36 @@ lbm_status lbm_run_streamed(lbm_handle *h, const float *moments, uint64_t n, voi
     const size_t pitch = h->N * sizeof(float);
     const int UP = std::min(P, 4);                                   // planes per upload chunk
     const int U = (nz + UP - 1) / UP;                                // upload chunks
+    // 16-bit storage: the host values (FP32) pass through a staging block of
+    // UP planes each way and a conversion kernel on the copy's own stream
+    float *stage_up = nullptr, *stage_down = nullptr;
+    if (h->storage != 0) {
+        const size_t sb = 10 * size_t(UP) * plane;
+        lbm_status ss = ensure_scratch(h, 2 * sb * sizeof(float));
+        if (ss != LBM_OK)
+            return ss;
+        stage_up = static_cast<float *>(h->scratch);
+        stage_down = stage_up + sb;
+    }
+    auto convert_planes = [&](bool in, float *stage, void *mbuf, size_t off, size_t cnt,
+                              cudaStream_t cs) -> lbm_status {
+        const dim3 g(unsigned(std::min<size_t>((cnt + 255) / 256, size_t(148) * 4)), 10);
+        if (h->storage == 1) {
+            if (in)
+                planes_in_kernel<<<g, 256, 0, cs>>>(static_cast<__half *>(mbuf), stage, h->N, off, cnt);
+            else
+                planes_out_kernel<<<g, 256, 0, cs>>>(stage, static_cast<const __half *>(mbuf), h->N, off, cnt);
+        } else {
+            if (in)
+                planes_in_kernel<<<g, 256, 0, cs>>>(static_cast<__nv_bfloat16 *>(mbuf), stage, h->N, off, cnt);
+            else
+                planes_out_kernel<<<g, 256, 0, cs>>>(stage, static_cast<const __nv_bfloat16 *>(mbuf), h->N, off,
+                                                     cnt);
+        }
+        LBM_CUDA(cudaGetLastError());
+        h->launches += 1;
+        return LBM_OK;
+    };
     const int in0 = h->cur;
     const int fin = int((uint64_t(in0) + n) & 1u);  // buffer of the final moments
     // A long job runs its first and last kSkew steps as skewed slabs (the
@@ -1159,11 +1207,22 @@ lbm_status lbm_run_streamed(lbm_handle *h, const float *moments, uint64_t n, voi
             LBM_CUDA(cudaEventRecord(done, h->stream));
             LBM_CUDA(cudaStreamWaitEvent(h->dstream, done, 0));
             const size_t z0 = size_t(flo), nzs = size_t(fhi - flo);
-            if (out[LBM_FIELDS_MOMENTS]) {
+            char *host_m = static_cast<char *>(out[LBM_FIELDS_MOMENTS]);
+            if (host_m && h->storage == 0) {
                 const size_t off = z0 * plane * sizeof(float);
-                LBM_CUDA(cudaMemcpy2DAsync(static_cast<char *>(out[LBM_FIELDS_MOMENTS]) + off, pitch,
-                                           static_cast<const char *>(h->m[fin]) + off, pitch,
+                LBM_CUDA(cudaMemcpy2DAsync(host_m + off, pitch, static_cast<const char *>(h->m[fin]) + off, pitch,
                                            nzs * plane * sizeof(float), 10, cudaMemcpyDeviceToHost, h->dstream));
+            } else if (host_m) {
+                for (size_t a = z0; a < z0 + nzs; a += size_t(UP)) {
+                    const size_t b = std::min(z0 + nzs, a + size_t(UP));
+                    const size_t off = a * plane, cnt = (b - a) * plane;
+                    lbm_status cs = convert_planes(false, stage_down, h->m[fin], off, cnt, h->dstream);
+                    if (cs != LBM_OK)
+                        return cs;
+                    LBM_CUDA(cudaMemcpy2DAsync(host_m + off * sizeof(float), pitch, stage_down,
+                                               cnt * sizeof(float), cnt * sizeof(float), 10, cudaMemcpyDeviceToHost,
+                                               h->dstream));
+                }
             }
             for (const Out &o : outs) {
                 const size_t off = z0 * plane * o.esz;
@@ -1192,9 +1251,18 @@ lbm_status lbm_run_streamed(lbm_handle *h, const float *moments, uint64_t n, voi
         char *dst0 = static_cast<char *>(h->m[in0]);
         for (int u = 0; u < U; u++) {
             const size_t z0 = size_t(u) * UP, z1 = std::min<size_t>(nz, z0 + UP);
-            const size_t off = z0 * plane * sizeof(float);
-            LBM_CUDA(cudaMemcpy2DAsync(dst0 + off, pitch, reinterpret_cast<const char *>(moments) + off, pitch,
-                                       (z1 - z0) * plane * sizeof(float), 10, cudaMemcpyHostToDevice, h->xstream));
+            const size_t off = z0 * plane, cnt = (z1 - z0) * plane;
+            const char *src = reinterpret_cast<const char *>(moments) + off * sizeof(float);
+            if (h->storage == 0) {
+                LBM_CUDA(cudaMemcpy2DAsync(dst0 + off * sizeof(float), pitch, src, pitch, cnt * sizeof(float), 10,
+                                           cudaMemcpyHostToDevice, h->xstream));
+            } else {
+                LBM_CUDA(cudaMemcpy2DAsync(stage_up, cnt * sizeof(float), src, pitch, cnt * sizeof(float), 10,
+                                           cudaMemcpyHostToDevice, h->xstream));
+                lbm_status cs = convert_planes(true, stage_up, dst0, off, cnt, h->xstream);
+                if (cs != LBM_OK)
+                    return cs;
+            }
             LBM_CUDA(cudaEventRecord(up[size_t(u)], h->xstream));
         }
         if (mon)

@@ -182,9 +182,10 @@ typedef struct lbm_stream_opts {
  * steps runs only its first and last 16 steps this way (with the upload and
  * the download respectively) and the steps between them as whole-mesh
  * launches.
- * Host buffers should be page-locked (lbm_host_alloc); the call returns when
- * the results are in host memory.  FP32 storage without the learned closure
- * (LBM_ERR_STATE otherwise).  Replaces: the reference's host-to-device copy
+ * With 16-bit storage the moments pass through small staging blocks and the
+ * storage conversion on the copy streams.  Host buffers should be
+ * page-locked (lbm_host_alloc); the call returns when the results are in
+ * host memory.  Not with the learned closure (LBM_ERR_STATE).  Replaces: the reference's host-to-device copy
  * of the initial state, time loop and device-to-host copies at save steps
  * (momentBasedD3Q19.cu:70-137, src/memory/memory.cuh:157-195), which run
  * one after the other. */
