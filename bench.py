@@ -337,12 +337,12 @@ def run_ours(args, w):
     if streamed:
         host_outs = {fs: b.array for fs, b in outs.items()}
         cav.run_streamed(state.array, min(args.steps, 4), host_outs, monitor=mon.array, slab=args.stream_slab,
-                         z_chunk=args.stream_zc)
+                         z_chunk=args.stream_zc, lead=args.stream_lead)
         barrier()
         cav.synchronize()
         t4 = time.perf_counter()
         cav.run_streamed(state.array, args.steps, host_outs, monitor=mon.array, slab=args.stream_slab,
-                         z_chunk=args.stream_zc)
+                         z_chunk=args.stream_zc, lead=args.stream_lead)
         t5 = time.perf_counter()
         barrier()
         e2e_s = max_over_ranks(t5 - t4)
@@ -776,6 +776,7 @@ def main():
                     help="plain workloads also timed (device) in the default run, comma-separated; '' for none")
     ap.add_argument("--stream-slab", type=int, default=0, help="lbm_run_streamed slab height (0: default)")
     ap.add_argument("--stream-zc", type=int, default=0, help="lbm_run_streamed z-chunk (0: default)")
+    ap.add_argument("--stream-lead", type=int, default=0, help="lbm_run_streamed first-slab lead (0: default)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -66,7 +66,7 @@ class Tuning(ctypes.Structure):
 
 
 class StreamOpts(ctypes.Structure):
-    _fields_ = [("slab", ctypes.c_int32), ("z_chunk", ctypes.c_int32)]
+    _fields_ = [("slab", ctypes.c_int32), ("z_chunk", ctypes.c_int32), ("lead", ctypes.c_int32)]
 
 
 class BatchInfo(ctypes.Structure):

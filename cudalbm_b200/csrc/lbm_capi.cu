@@ -1067,8 +1067,9 @@ lbm_status lbm_run_streamed(lbm_handle *h, const float *moments, uint64_t n, voi
         return fail(LBM_ERR_STATE, "lbm_run_streamed: not available with the learned closure");
     const int P = opts && opts->slab > 0 ? opts->slab : 16;
     const int zc = opts && opts->z_chunk > 0 ? std::min(opts->z_chunk, P) : std::min(4, P);
-    if (P > (1 << 20))
-        return fail(LBM_ERR_ARG, "lbm_run_streamed: slab too large");
+    const int lead = opts && opts->lead > 0 ? opts->lead : 2;
+    if (P > (1 << 20) || lead > (1 << 20))
+        return fail(LBM_ERR_ARG, "lbm_run_streamed: slab or lead too large");
     // host buffers and the device field of every requested set
     struct Out {
         char *host;
@@ -1169,12 +1170,12 @@ lbm_status lbm_run_streamed(lbm_handle *h, const float *moments, uint64_t n, voi
     int waited = -1;  // upload chunks the compute stream has waited for
     // Steps [s0, s0 + m) as skewed slabs: slab j covers planes [bnd(j),
     // bnd(j+1)) at its first step and one plane lower at each following
-    // step; the first slab is m + P/2 planes high, so that its own last step
-    // already finishes planes, the others P, up to nz + m - 1.  With
+    // step; the first slab is m + lead planes high, so that its own last
+    // step already finishes planes, the others P, up to nz + m - 1.  With
     // `uploads`, slab j first waits for the chunk that holds plane bnd(j+1);
     // with `downloads`, the planes slab j finished go to the host after it.
     auto skewed = [&](uint64_t s0, uint64_t m, bool uploads, bool downloads) -> lbm_status {
-        const int64_t F = int64_t(m) + P / 2;
+        const int64_t F = int64_t(m) + lead;
         auto bnd = [&](int64_t j) -> int64_t { return j == 0 ? 0 : F + (j - 1) * int64_t(P); };
         const int64_t span = int64_t(nz) + int64_t(m) - 1;
         const int J = int(1 + (span > F ? (span - F + P - 1) / P : 0));

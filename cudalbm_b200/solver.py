@@ -176,7 +176,7 @@ class Cavity:
         return out
 
     def run_streamed(self, moments: np.ndarray, n: int, outs: Dict[str, np.ndarray], monitor=None,
-                     slab: int = 0, z_chunk: int = 0) -> None:
+                     slab: int = 0, z_chunk: int = 0, lead: int = 0) -> None:
         """One job between host arrays with the copies overlapping the steps:
         upload ``moments`` ([10, nz, ny, nx] float32), advance ``n`` steps and
         download each field set named in ``outs`` into its array ([nvars, nz,
@@ -195,7 +195,7 @@ class Cavity:
             ptrs[_lib.FIELD_SET[name]] = arr.ctypes.data
         if monitor is not None and (monitor.dtype != np.dtype(_lib.MONITOR_DTYPE) or monitor.size < n):
             raise ValueError("monitor must be a MONITOR_DTYPE array of at least n entries")
-        opts = _lib.StreamOpts(int(slab), int(z_chunk))
+        opts = _lib.StreamOpts(int(slab), int(z_chunk), int(lead))
         _lib.check(_lib.lib().lbm_run_streamed(self._h, moments.ctypes.data, int(n), ptrs,
                                                monitor.ctypes.data if monitor is not None else None,
                                                ctypes.byref(opts)))

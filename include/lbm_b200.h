@@ -157,6 +157,7 @@ lbm_status lbm_step_monitored(lbm_handle *h, uint64_t n, lbm_monitor *out);
 typedef struct lbm_stream_opts {
     int32_t slab;      /* planes per slab (default 16) */
     int32_t z_chunk;   /* planes per CTA inside a slab launch (default 4) */
+    int32_t lead;      /* the first slab is n + lead planes high (default 2) */
 } lbm_stream_opts;
 
 /* One whole job between host buffers, with the transfers overlapped with
@@ -171,7 +172,7 @@ typedef struct lbm_stream_opts {
  * moments.  The results are those of lbm_write_fields + lbm_step(n) +
  * lbm_read_fields, bit for bit (the monitor sums up to FP64 summation
  * order).
- * How: the mesh is cut into z-slabs (the first n + slab/2 planes high, so
+ * How: the mesh is cut into z-slabs (the first n + lead planes high, so
  * that its own last step already finishes planes, the others `slab`); slab j
  * of step s is shifted down by s planes, so that it needs only slabs j-1 and
  * j of step s-1, and all n steps of slab j run before slab j+1.  The upload
