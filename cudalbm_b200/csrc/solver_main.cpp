@@ -191,6 +191,11 @@ int run(int argc, char **argv)
     cfg.function_objects = lbm::read_function_objects(".");
     cfg.start_step = int64_t(latest);
     bool restore_means = false;
+    // kernel shape: the autotuner times the compiled variants on this run's
+    // own state and restores it (every variant computes the same bits); by
+    // default only for runs long enough to repay the trial steps
+    const uint64_t steps_to_run = pc.nTimeSteps > latest ? pc.nTimeSteps - latest : 0;
+    bool autotune = steps_to_run >= 1000;
     if (std::filesystem::exists("b200Options")) {
         const lbm::Lines L = lbm::read_lines("b200Options");
         try {
@@ -199,6 +204,10 @@ int run(int argc, char **argv)
         }
         try {
             restore_means = std::stoi(lbm::parameter_string(L, "restoreMeans")) != 0;
+        } catch (const lbm::CaseError &) {
+        }
+        try {
+            autotune = std::stoi(lbm::parameter_string(L, "autotune")) != 0;
         } catch (const lbm::CaseError &) {
         }
     }
@@ -224,6 +233,14 @@ int run(int argc, char **argv)
     } else {
         const std::array<float, 70> region = lbm::read_initial_conditions(".");
         check(lbm_init_regions(h, region.data()));
+    }
+
+    if (autotune) {
+        // a failure here (e.g. no room for the state copy the trials need)
+        // leaves the default shape in place
+        lbm_tuning tuning;
+        if (lbm_autotune(h, 10, &tuning) != LBM_OK)
+            std::cerr << "autotune skipped: " << lbm_last_error() << std::endl;
     }
 
     const Saver save{h, mesh, N, cfg.function_objects, cfg.mean_bits};

@@ -127,3 +127,23 @@ def test_restart_without_restored_means_keeps_the_reference_behaviour():
     assert not np.array_equal(ma, mb)
     # after the restart the means hold only steps 20..39, weighted by 1/(t+1)
     assert np.abs(mb).max() < np.abs(ma).max()
+
+
+@pytest.mark.parametrize("q", [19, 27])
+def test_autotuned_run_writes_the_same_files(q):
+    """b200Options `autotune 1;` (the default from 1000 steps on) times the
+    kernel shapes on the run's own state before the loop; the files are
+    those of the default shape, byte for byte."""
+    spec = casefiles.CaseSpec(nx=32, ny=32, nz=40, Re=500.0, u_inf=0.05, n_steps=41, save_interval=20,
+                              info_interval=20, function_objects=("S", "SMean", "k", "kMean"))
+    plain, tuned = tempfile.mkdtemp(), tempfile.mkdtemp()
+    for d, flag in ((plain, 0), (tuned, 1)):
+        casefiles.write_case(d, spec)
+        with open(os.path.join(d, "b200Options"), "w") as fh:
+            fh.write(f"autotune {flag};\n")
+        out = run(os.path.join(BIN, f"momentBasedD3Q{q}"), d)
+        assert "autotune skipped" not in out.stderr
+    files = lbmbin_files(plain)
+    assert files and lbmbin_files(tuned) == files
+    for f in files:
+        assert open(os.path.join(plain, f), "rb").read() == open(os.path.join(tuned, f), "rb").read(), f
