@@ -5,6 +5,7 @@
 
 Outputs:
   cudalbm_b200/lib/liblbm_b200.so      C ABI of include/lbm_b200.h (sm_100a)
+  cudalbm_b200/lib/liblbm_b200_checked.so  the same, its step kernels checking every index (tests)
   cudalbm_b200/bin/momentBasedD3Q19    solver executables with the reference's
   cudalbm_b200/bin/momentBasedD3Q27    command line and case files
   cudalbm_b200/bin/fieldConvert        .LBMBin -> VTS (whole fields or cut planes)
@@ -23,6 +24,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "lib", "liblbm_b200.so")
+LIB_CHECKED = os.path.join(HERE, "lib", "liblbm_b200_checked.so")  # step kernels with index checks
 BIN = os.path.join(HERE, "bin")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -56,25 +58,42 @@ def _run(cmd):
     subprocess.run(cmd, check=True)
 
 
-def build_library(force: bool = False, verbose_ptxas: bool = False) -> str:
-    """Compile every source to an object in parallel, then link the library."""
-    from concurrent.futures import ThreadPoolExecutor
-
-    if not (force or _stale(LIB, _deps())):
-        return LIB
-    objdir = os.path.join(HERE, "lib", "obj")
+def _library_jobs(checked: bool, verbose_ptxas: bool = False):
+    """(compile commands, objects, link command, output) of the library or of
+    its checked build (-DLBM_CHECKED: the step kernels verify their indices)."""
+    lib = LIB_CHECKED if checked else LIB
+    objdir = os.path.join(HERE, "lib", "obj_checked" if checked else "obj")
     os.makedirs(objdir, exist_ok=True)
+    flags = NVCC_FLAGS + (["-DLBM_CHECKED"] if checked else [])
     jobs = []
     for src in LIB_SOURCES:
         obj = os.path.join(objdir, src + ".o")
-        cmd = [_nvcc()] + NVCC_FLAGS + ["-c", os.path.join(CSRC, src), "-o", obj]
+        cmd = [_nvcc()] + flags + ["-c", os.path.join(CSRC, src), "-o", obj]
         if verbose_ptxas:
             cmd += ["-Xptxas", "-v"]
         jobs.append((cmd, obj))
+    link = [_nvcc()] + flags + ["-shared"] + [o for _, o in jobs] + ["-o", lib + ".tmp"]
+    return jobs, link, lib
+
+
+def build_library(force: bool = False, verbose_ptxas: bool = False, checked_too: bool = True) -> str:
+    """Compile every source to an object in parallel (the library and, with
+    checked_too, its checked build), then link."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    builds = []
+    for checked in ((False, True) if checked_too else (False,)):
+        lib = LIB_CHECKED if checked else LIB
+        if force or _stale(lib, _deps()):
+            builds.append(_library_jobs(checked, verbose_ptxas))
+    if not builds:
+        return LIB
+    jobs = [j for b in builds for j in b[0]]
     with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as pool:
         list(pool.map(lambda j: _run(j[0]), jobs))
-    _run([_nvcc()] + NVCC_FLAGS + ["-shared"] + [o for _, o in jobs] + ["-o", LIB + ".tmp"])
-    os.replace(LIB + ".tmp", LIB)
+    for _, link, lib in builds:
+        _run(link)
+        os.replace(lib + ".tmp", lib)
     return LIB
 
 

@@ -601,6 +601,13 @@ EncodeTiledFn encode_tiled() { return get_encode(); }
 
 lbm_status check_fault(const StepFault &f, const char *who)
 {
+    if (f.flags & ERR_BOUNDS) {
+        // only the checked build (LBM_CHECKED) sets this flag
+        char buf[256];
+        std::snprintf(buf, sizeof(buf), "%s failed index check %u (block %d,%d,%d item %d mesh %d plane %d)", who,
+                      f.slot, f.block[0], f.block[1], f.block[2], f.item, f.mesh, f.plane);
+        return fail(LBM_ERR_STATE, buf);
+    }
     if (f.flags & ERR_MMA_TIMEOUT)
         return fail(LBM_ERR_TIMEOUT, "the closure network timed out waiting for a tensor-core MMA");
     if (!(f.flags & ERR_TMA_TIMEOUT))

@@ -386,6 +386,49 @@ static __device__ __noinline__ void record_fault(StepFault *f, unsigned flag, in
     }
 }
 
+// ---------------------------------------------------------- checked build
+// With LBM_CHECKED (the separately built checked library, the stand-in for a
+// memory checker on this hardware) the step kernels verify every shared-
+// memory index, global node index and TMA coordinate before they use it.  A
+// failed check sets ERR_BOUNDS in the fault record, with the check's number
+// in `slot` and the place (block, item, plane), replaces a shared-memory
+// index by 0 and skips a global store, so nothing outside the buffers is
+// touched; lbm_synchronize then reports LBM_ERR_STATE.  The ordinary build
+// compiles the checks away.
+enum : unsigned { ERR_BOUNDS = 4u };
+enum : unsigned { CHK_TMA_X = 1, CHK_TMA_PLANE = 2, CHK_STAGE = 3, CHK_POP = 4, CHK_NODE = 5, CHK_PTR = 6 };
+
+static __device__ __noinline__ void record_bounds(StepFault *f, unsigned code, int item, int mesh, int plane,
+                                                  unsigned seq)
+{
+    atomicOr(&f->flags, ERR_BOUNDS);
+    if (atomicCAS(&f->recorded, 0u, 2u) == 0u) {
+        f->block[0] = blockIdx.x;
+        f->block[1] = blockIdx.y;
+        f->block[2] = blockIdx.z;
+        f->item = item;
+        f->mesh = mesh;
+        f->plane = plane;
+        f->seq = seq;
+        f->slot = code;
+        f->parity = 0;
+        f->barrier = 0;
+        __threadfence();
+        atomicExch(&f->recorded, 1u);
+    }
+}
+
+#ifdef LBM_CHECKED
+// cond holds, or the failure is recorded (false)
+#define LBM_CHK(cond, code, plane) \
+    ((cond) ? true : (record_bounds(p.fault, (code), item, mesh, (plane), g0 + unsigned(plane)), false))
+// idx if 0 <= idx < limit, else 0 (and the failure recorded)
+#define LBM_IDX(idx, limit, plane) (LBM_CHK((idx) >= 0 && (idx) < (limit), CHK_POP, plane) ? (idx) : 0)
+#else
+#define LBM_CHK(cond, code, plane) true
+#define LBM_IDX(idx, limit, plane) (idx)
+#endif
+
 // One work item: tile (bx, by) of the x-y plane, z-chunk bz of the mesh that
 // p and tmap describe.  The planes a CTA receives are numbered g0, g0+1, ...
 // across all the items it processes, so that the stage slot (g % NSTAGE), the
@@ -433,6 +476,20 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
     static_assert(PG::d_plane(PG::NG) == XY<Q>::N, "population-plane groups cover the x-y movers");
     constexpr bool FO4 = FO == 2;  // S, SMean, k, kMean present, momentsMean absent
     const int my_cell = (ty + 1) * G::PX + tx + 1;
+    constexpr int PCELLS = G::PX * G::PY;  // cells of one population-plane group
+#ifdef LBM_CHECKED
+    {
+        // the TMA box starts 16-byte aligned in x; the item's planes lie in
+        // the mesh; the staged plane holds this thread's row and column; the
+        // output and function-object buffers the kernel writes exist
+        (void)LBM_CHK(((x0 - G::XPAD) * Storage<ST>::BYTES) % 16 == 0, CHK_TMA_X, 0);
+        (void)LBM_CHK(z0 >= 0 && z0 < z1 && z1 <= p.nz && z0 >= p.z_lo && z1 <= p.z_hi, CHK_TMA_PLANE, 0);
+        (void)LBM_CHK(ty + 1 < G::RY && tx + G::XPAD < G::TXP, CHK_STAGE, 0);
+        (void)LBM_CHK(p.out != nullptr && (!MON || p.mon != nullptr) &&
+                          (!FO4 || (p.fo.S && p.fo.SMean && p.fo.k && p.fo.kMean)),
+                      CHK_PTR, 0);
+    }
+#endif
 
     // first planes of the item (the slots were last read by ordinary loads)
 #pragma unroll
@@ -470,14 +527,18 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
         const uint32_t iu = uint32_t(zu) * plane32 + row32;
         MeanT sm_old[6], km_old = MeanT(0);
         float dtau = 0.0f;
+        // this thread updates a node in this iteration (checked build: one in
+        // this launch's planes and in the mesh); only such threads touch the
+        // node's global fields
+        const bool upd_node = upd && own && LBM_CHK(zu >= p.z_lo && zu < p.z_hi && size_t(iu) < N, CHK_NODE, i);
         if constexpr (CLM == 1) {
-            if (upd)
+            if (upd_node)
                 dtau = p.dtau[iu];
         }
         // the network runs for the planes this CTA updates (z0 .. z1-1)
         const bool net_plane = (i >= 1) && (i <= nplanes - 2);
         if constexpr (FO != 0) {
-            if (upd) {
+            if (upd_node) {
                 if (FO4 || p.fo.SMean) {
 #pragma unroll
                     for (int c = 0; c < 6; c++)
@@ -510,11 +571,34 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
             }
             m[0] = rho_of_stored<ST>(m[0]);
             const RecPre r = rec_pre<Q, Storage<ST>::SCI>(m);
-            static_for<0, PG::NG>([&](auto gc) { store_group<Q, TX, TY, ST, decltype(gc)::value>(pb, my_cell, r, m); });
+            const int cell = LBM_IDX(my_cell, PCELLS, i);
+            static_for<0, PG::NG>([&](auto gc) { store_group<Q, TX, TY, ST, decltype(gc)::value>(pb, cell, r, m); });
             own_up = rec_q<Q, 5>(r, m);
             D0[zslot<Q>(6)] = rec_q<Q, 6>(r, m);
             own_rest = rec_q<Q, 0>(r, m);
         }
+#ifdef LBM_CHECKED
+        {
+            // every ring node this thread reconstructs lies on the ring
+            int rx = -2, ry = -2;
+            if (TX == 32) {
+                const int w = lin >> 5, l = lin & 31;
+                if (w == 0) { rx = l; ry = -1; }
+                else if (w == 1) { rx = l; ry = TY; }
+                else if (w == 2 && l < TY + 2) { rx = -1; ry = l - 1; }
+                else if (w == 3 && l < TY + 2) { rx = TX; ry = l - 1; }
+            } else if (lin < G::RING) {
+                int r = lin;
+                if (r < TX + 2) { rx = r - 1; ry = -1; }
+                else if ((r -= TX + 2) < TX + 2) { rx = r - 1; ry = TY; }
+                else if ((r -= TX + 2) < TY) { rx = -1; ry = r; }
+                else { rx = TX; ry = r - TY; }
+            }
+            if (rx != -2)
+                (void)LBM_CHK(rx >= -1 && rx <= TX && ry >= -1 && ry <= TY && (rx == -1 || rx == TX || ry == -1 || ry == TY),
+                              CHK_POP, i);
+        }
+#endif
         // ring nodes: only the directions that enter the tile.  With 32-wide
         // tiles each side goes to one warp (the bottom and top rows, x = 0..31,
         // to warps 0 and 1; the left and right columns, corners included, to
@@ -556,6 +640,7 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
         }
 
         // the stage is consumed: refill it with plane i + NSTAGE
+        (void)LBM_CHK(!(lin == 0 && i + NSTAGE < nplanes) || (pz + NSTAGE <= p.nz && pz + NSTAGE <= z1), CHK_TMA_PLANE, i);
         tma_issue_if(lin == 0 && i + NSTAGE < nplanes, sm, tmap, x0 - G::XPAD, y0 - 1, pz + NSTAGE, 0, &bars[stage],
                      G::PLANE_BYTES);
 
@@ -566,7 +651,7 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
             constexpr int off = group_cy(g) * G::PX + group_cx(g);
             if constexpr (qd >= 0) {
                 constexpr int sd = zslot<Q>(qd);
-                D0[sd] = pb[C::template d<g>(my_cell - off)];
+                D0[sd] = pb[C::template d<g>(LBM_IDX(my_cell - off, PCELLS, i))];
             }
         });
 
@@ -589,7 +674,7 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
                 if constexpr (c == 0) f[q] = S1[zslot<Q>(q)];
                 if constexpr (c == -1) f[q] = D0[zslot<Q>(q)];
             });
-            if (own) {
+            if (upd_node) {
                 const unsigned type = type_xy | (zu == 0 ? BACK : 0u) | (zu == p.nz - 1 ? FRONT : 0u);
                 float m[10];
                 if constexpr (CLM != 0) {
@@ -673,7 +758,7 @@ __device__ __forceinline__ bool march_chunk(const CUtensorMap *tmap, const StepP
             constexpr int off = group_cy(g) * G::PX + group_cx(g);
             constexpr int qs = PG::qS(g), qu = PG::qU(g);
             constexpr int ss = zslot<Q>(qs);
-            const int cell = my_cell - off;
+            const int cell = LBM_IDX(my_cell - off, PCELLS, i);
             if constexpr (qu >= 0) {
                 constexpr int su_slot = zslot<Q>(qu);
                 const float2 su = *reinterpret_cast<const float2 *>(pb + C::template su<g>(cell));
