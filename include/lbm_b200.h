@@ -186,7 +186,9 @@ typedef struct lbm_stream_opts {
  * With 16-bit storage the moments pass through small staging blocks and the
  * storage conversion on the copy streams.  Host buffers should be
  * page-locked (lbm_host_alloc); the call returns when the results are in
- * host memory.  Not with the learned closure (LBM_ERR_STATE).  Replaces: the reference's host-to-device copy
+ * host memory.  Not with the learned closure (LBM_ERR_STATE).  After a
+ * failure the handle's moments are those of some mix of steps: write a state
+ * again before stepping on.  Replaces: the reference's host-to-device copy
  * of the initial state, time loop and device-to-host copies at save steps
  * (momentBasedD3Q19.cu:70-137, src/memory/memory.cuh:157-195), which run
  * one after the other. */
