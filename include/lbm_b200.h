@@ -79,7 +79,8 @@ typedef struct lbm_config {
     int64_t start_step;       /* absolute step index of the initial state (restart: latestTime) */
     /* kernel tiling; 0 = autotuned choice for this size class */
     int32_t tile_x, tile_y, z_chunk, stages;
-    int32_t pop_buffers;      /* shared-memory population planes: 2 (one barrier per plane) or 1 */
+    int32_t pop_buffers;      /* shared-memory population planes: 1 (two barriers per plane, 3 CTAs/SM),
+                                 2 (one barrier per plane), 4 (one plane, 4 CTAs/SM; D3Q19 shapes) */
     int32_t storage;          /* LBM_STORAGE_*: how the 10 moment fields are held in device memory */
 } lbm_config;
 
