@@ -332,21 +332,18 @@ def run_ours(args, w):
     # (b) the same job as one lbm_run_streamed call: the upload, the steps
     # and the download overlap (z-slabs of each step shifted by the step
     # index).  One untimed call first (streams, events, staging).
-    streamed = True
-    e2e_s = seq_s
-    if streamed:
-        host_outs = {fs: b.array for fs, b in outs.items()}
-        cav.run_streamed(state.array, min(args.steps, 4), host_outs, monitor=mon.array, slab=args.stream_slab,
-                         z_chunk=args.stream_zc, lead=args.stream_lead)
-        barrier()
-        cav.synchronize()
-        t4 = time.perf_counter()
-        cav.run_streamed(state.array, args.steps, host_outs, monitor=mon.array, slab=args.stream_slab,
-                         z_chunk=args.stream_zc, lead=args.stream_lead)
-        t5 = time.perf_counter()
-        barrier()
-        e2e_s = max_over_ranks(t5 - t4)
-        red = {"mass": float(mon.array[-1]["mass"]), "nonfinite": int(mon.array["nonfinite"].max())}
+    host_outs = {fs: b.array for fs, b in outs.items()}
+    cav.run_streamed(state.array, min(args.steps, 4), host_outs, monitor=mon.array, slab=args.stream_slab,
+                     z_chunk=args.stream_zc, lead=args.stream_lead)
+    barrier()
+    cav.synchronize()
+    t4 = time.perf_counter()
+    cav.run_streamed(state.array, args.steps, host_outs, monitor=mon.array, slab=args.stream_slab,
+                     z_chunk=args.stream_zc, lead=args.stream_lead)
+    t5 = time.perf_counter()
+    barrier()
+    e2e_s = max_over_ranks(t5 - t4)
+    red = {"mass": float(mon.array[-1]["mass"]), "nonfinite": int(mon.array["nonfinite"].max())}
     e2e = world * nodes * args.steps / e2e_s / 1e6
     cav.close()
     group.close()
@@ -382,13 +379,11 @@ def run_ours(args, w):
                 "d2h_bytes_per_step": round(24 + d2h / args.steps),
                 "what": ("one lbm_run_streamed call: pinned h2d of the state, K steps (each step's 24 B FP64 "
                          "mass/energy/non-finite sums), d2h of the moments and function objects, the copies "
-                         "overlapping the steps" if streamed else
-                         "lbm_write_fields (pinned h2d of the state) + K x lbm_step_monitored (each step's 24 B "
-                         "FP64 mass/energy/non-finite sums copied back) + lbm_read_fields of moments and "
-                         "function objects"),
+                         "overlapping the steps"),
                 "seconds": round(e2e_s, 5),
                 "sequential": {"value": round(world * nodes * args.steps / seq_s / 1e6, 2),
-                               "what": "the same transfers and steps as separate calls, one after the other",
+                               "what": ("the same job as separate calls, one after the other: lbm_write_fields, "
+                                        "K x lbm_step_monitored, lbm_read_fields of moments and function objects"),
                                "seconds": {"h2d": round(t1 - t0, 5), "steps": round(t2 - t1, 5),
                                            "d2h": round(t3 - t2, 5)},
                                "copy_gbs": copy_gbs},
